@@ -1,0 +1,391 @@
+#!/usr/bin/env python3
+"""Benchmark: particle-steps/s of the Barnes-Hut evolution step on B200.
+
+Workload (one GPU): cold collapse of a uniform unit disc, N = 2^20 equal
+masses (total 1, G = 1), f32 state, eps = 0.005, theta = 0.5, bucket 1,
+32-bit Morton codes, full tree rebuild every step, KDK leapfrog dt = 5e-4,
+seed 7.  One "step" = kick/drift + bounds + Morton + stable radix sort +
+topology + aggregates + theta-MAC traversal + final kick over all bodies.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line (rank 0).  With N > 1 (launched by torchrun) every rank
+advances its own replica of the workload (the path does not shard: replicas
+only, weak scaling); time is the max over ranks.  ``--impl reference`` times
+the reference's CPU flat-tree evolution (its C restatement, all host
+threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BODIES = 1 << 20
+THETA, EPS, G, BUCKET, DT, SEED = 0.5, 0.005, 1.0, 1, 5e-4, 7
+METRIC = "particle-steps/s"
+WORKLOAD = "cold-collapse uniform disc N=2^20, eps=0.005, theta=0.5, bucket=1, dt=5e-4, seed 7"
+
+def algorithmic_bytes(c: float) -> dict:
+    """Bytes each HBM-bound stage must move per body (reads + writes),
+    counted from the records it touches; c = cells per body (measured)."""
+    return {
+        # kick/drift: read 32 B state + 16 B accel, write 32 B state
+        "integrate": 80.0,
+        # Morton: read x,y (8 B), write 4 B code
+        "morton": 12.0,
+        # radix: pass 0 reads 4 B key, writes 8 B; passes 1-3 read 8 B write 8 B;
+        # last pass gathers 16 B of state and writes a 16 B sorted body
+        "radix": 4 + 8 + 3 * 16 + 16 + 16,
+        # count+scan reads codes (4 B) writes base (4 B); cells read codes/base
+        # and write 16 B range + 16 B children + 4 B parent + 4 B counter per cell
+        "topology": 8 + 8 + c * 40.0,
+        # aggregate: sorted bodies 16 B + base 8 B; per cell read 16 B range +
+        # 16 B children + 4 B parent + 4 B counter, write 32 B f64 + 16 B f32
+        "aggregate": 24 + c * 88.0,
+    }
+
+
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured", "sm_max_mhz": d.get("sm_max_mhz")}
+    return {"hbm_gbs": 6650.0, "source": "fallback", "sm_max_mhz": 1965.0}
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def f32_workload():
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import bodies_to_state
+    bodies = scenarios.cold_disc(N_BODIES, SEED)
+    return bodies, bodies_to_state(bodies)
+
+
+# ------------------------------------------------------------ reference --
+
+def run_reference(args, world, rank, pg):
+    """The reference's CPU flat-tree evolution (cpu_flat_evolve,
+    galaxy-bh-evolve.rs:339-363) through its C restatement, all host threads,
+    on the same workload.  Each step is one full KDK step at N = 2^20; the
+    timed steps stop early at a 150 s budget and the rate covers the steps
+    that ran."""
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    from galaxy_b200.nbody_gpu import state_to_bodies
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    _, s = f32_workload()
+    b = np.ascontiguousarray(state_to_bodies(s))
+    cfg = oracle.Config(theta=THETA, softening=EPS, g=G, bucket=BUCKET, max_depth=48)
+    tree = oracle.build_flat_tree(b, cfg)
+    acc, _ = oracle.flat_accelerations(b, tree, cfg, nthreads=threads)
+    acc = np.ascontiguousarray(acc)
+    for _ in range(min(args.warmup, 1)):
+        oracle.cpu_flat_steps(b, acc, 1, DT, cfg, threads)
+    t0 = time.perf_counter()
+    done = 0
+    tb = tf = 0.0
+    while done < args.steps:
+        b1, f1 = oracle.cpu_flat_steps(b, acc, 1, DT, cfg, threads)
+        tb += b1
+        tf += f1
+        done += 1
+        if time.perf_counter() - t0 > 150.0:
+            break
+    secs = time.perf_counter() - t0
+    value = N_BODIES * done / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+        "n_gpus": args.gpus, "steps": done, "warmup": min(args.warmup, 1),
+        "ms_per_step": 1e3 * secs / done, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_bodies": N_BODIES, "parallelism": "cpu threads"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{done} KDK steps at N=2^20 (of {args.steps} requested; "
+                                   f"150 s budget); tree build {tb:.2f} s single-threaded, "
+                                   f"forces {tf:.2f} s on {threads} threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+# --------------------------------------------------------------- engine --
+
+def cpu_baseline_sample() -> dict:
+    """One single-threaded KDK step of the oracle at the full workload size
+    (the reference CPU path is single-threaded)."""
+    from galaxy_b200.nbody_gpu import state_to_bodies
+    from oracle import oracle
+    _, s = f32_workload()
+    b = np.ascontiguousarray(state_to_bodies(s))
+    cfg = oracle.Config(theta=THETA, softening=EPS, g=G, bucket=BUCKET, max_depth=48)
+    tree = oracle.build_flat_tree(b, cfg)
+    acc, _ = oracle.flat_accelerations(b, tree, cfg, nthreads=os.cpu_count() or 1)
+    acc = np.ascontiguousarray(acc)
+    t0 = time.perf_counter()
+    tb, tf = oracle.cpu_flat_steps(b, acc, 1, DT, cfg, 1)
+    secs = time.perf_counter() - t0
+    return {"value": N_BODIES / secs, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"1 KDK step at N=2^20, single thread (tree build {tb:.2f} s, "
+                      f"forces {tf:.2f} s)"}
+
+
+def run_engine(args, world, rank, local, pg):
+    import torch
+
+    from galaxy_b200 import _lib
+    from galaxy_b200.nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime
+
+    torch.cuda.set_device(local)
+    gpu = NbodyGpu(str(local))
+    rt = ParallelTreeRuntime(gpu)
+    cfg = Config(theta=THETA, softening_kpc=EPS, g=G, bucket=BUCKET, max_depth=48)
+    bodies, s0 = f32_workload()
+    ev, _ = gpu.create_evolving_state_records(s0)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    stream = torch.cuda.ExternalStream(gpu.stream_ptr(), device=torch.device("cuda", local))
+
+    rt.step(gpu, ev, tree, cfg, DT, max(args.warmup, 3))
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        e0.record(stream)
+        rt.step(gpu, ev, tree, cfg, DT, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+        pg.barrier()
+    value = world * N_BODIES * args.steps / (ms * 1e-3)
+
+    # --- per-stage device times (instrumented rebuild + force, same state)
+    reps = 5
+    stage = {"bounds": 0.0, "morton": 0.0, "radix": 0.0, "topology": 0.0, "aggregate": 0.0,
+             "traverse": 0.0}
+    for _ in range(reps):
+        bt = rt.rebuild(gpu, ev, tree, cfg)
+        ft = rt.force(gpu, ev, tree, cfg)
+        stage["bounds"] += bt.bounds_seconds / reps
+        stage["morton"] += bt.morton_seconds / reps
+        stage["radix"] += bt.radix_seconds / reps
+        stage["topology"] += bt.topology_seconds / reps
+        stage["aggregate"] += bt.aggregate_seconds / reps
+        stage["traverse"] += ft.dispatch_seconds / reps
+    fstats = rt.force_stats(gpu, tree)
+    evid_meta_cells = tree_cells(gpu, rt, tree)
+    c = evid_meta_cells / N_BODIES
+    ab = algorithmic_bytes(c)
+    peaks = load_peaks()
+    # sort/build/leapfrog: every HBM-bound stage of the step
+    hbm_bytes = N_BODIES * sum(ab.values())
+    hbm_secs = stage["bounds"] + stage["morton"] + stage["radix"] + stage["topology"] + \
+        stage["aggregate"]
+    achieved = hbm_bytes / hbm_secs / 1e9
+    interactions = fstats["approximated_cells"] + fstats["direct_terms"]
+    flops = 20.0 * interactions
+    clk = clocks.summary()
+    sm_mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+
+    # --- end to end through the public API with host buffers
+    e2e_steps = min(args.steps, 20)
+    pinned = torch.empty(N_BODIES * 32, dtype=torch.uint8, pin_memory=True)
+    host = pinned.numpy().view(_lib.EVOLVE_STATE_DTYPE)
+    gpu_state, _ = gpu.read_evolving_state_records(ev)
+    host[:] = gpu_state
+    L = _lib.load()
+    hp = host.ctypes.data
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        _lib.check(L.galaxy_bh_write_state(gpu.handle, ev.handle, hp, N_BODIES))
+        rt.step(gpu, ev, tree, cfg, DT, 1)
+        _lib.check(L.galaxy_bh_read_state(gpu.handle, ev.handle, hp, N_BODIES, None))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = time.perf_counter() - t0
+    e2e_ms = e0.elapsed_time(e1)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * N_BODIES * e2e_steps / (e2e_ms * 1e-3)
+
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline else cpu_baseline_sample()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded cold uniform disc)",
+        "config": {"workload": WORKLOAD, "n_bodies": N_BODIES, "theta": THETA, "eps": EPS,
+                   "bucket": BUCKET, "dt": DT, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (state 32 MiB + accel 16 MiB + sort 24 MiB + "
+                         f"cells {evid_meta_cells * 104 / 2**20:.0f} MiB per step)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "kernels": "sort/build/leapfrog (integrate+bounds, morton, 4 radix "
+                                "passes, count/scan, cells, aggregate)",
+                     "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_body": {k: round(v, 1) for k, v in ab.items()},
+                     "stage_ms": {k: round(v * 1e3, 4) for k, v in stage.items()}},
+        "traversal": {"bound": "fp32", "interactions_per_step": interactions,
+                      "interactions_per_s": interactions / stage["traverse"],
+                      "achieved_tflops": flops / stage["traverse"] / 1e12,
+                      "peak_tflops": fp32_peak, "peak_source": "nominal FP32 at sampled clock",
+                      "frac": flops / stage["traverse"] / 1e12 / fp32_peak,
+                      "share_of_step": stage["traverse"] / (ms * 1e-3 / args.steps),
+                      "cells_per_body": c, "exact_mac_fallbacks": fstats["exact_mac_fallbacks"]},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 32 * N_BODIES,
+                "d2h_bytes_per_step": 32 * N_BODIES, "steps": e2e_steps,
+                "how": "per step: galaxy_bh_write_state from pinned host, one fused KDK step, "
+                       "galaxy_bh_read_state to pinned host (C ABI)",
+                "wall_s": e2e_wall},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": 10 * args.steps + 1,
+        "gpu": gpu.info().get("name"),
+    }
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def tree_cells(gpu, rt, tree) -> int:
+    import ctypes as C
+
+    from galaxy_b200 import _lib
+    cnt = C.c_uint32()
+    _lib.check(_lib.load().galaxy_bh_read_tree_evidence(gpu.handle, tree.handle, None, None,
+                                                         None, 0, None, 0, C.byref(cnt)))
+    return int(cnt.value)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, pg)
+    else:
+        run_engine(args, world, rank, local, pg)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,124 @@
+// SPDX-License-Identifier: Apache-2.0
+// Internal types shared by the engine's kernels and its host runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/galaxy_bh.h"
+
+namespace gbh {
+
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kChunk = 32;  // positions per warp chunk; sims start on a chunk boundary
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 8;
+constexpr uint32_t kTile = kSortThreads * kSortItems;  // keys per radix tile (2048)
+constexpr int kRadixDigits = 256;
+constexpr int kRadixPasses = 4;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // positions per scan tile
+constexpr uint32_t kMortonDepth = 16;
+
+// Error bits accumulated in the device error word until the host reads it.
+enum : uint32_t {
+    kErrLookbackTimeout = 1u,
+    kErrCapacity = 2u,
+    kErrTraversal = 4u,
+    kErrPackedStack = 8u,
+    kErrPackedIndex = 16u,
+};
+
+// One simulation of a batch (the plain path is a batch of one).
+struct SimDesc {
+    GpuEvolveState* state;  // resident state, n records (resident order)
+    float4* accel;          // resident accelerations, n records
+    float* potential;       // optional per-body softened potential (n) or null
+    uint32_t off;           // first position in the batch position space (multiple of 32)
+    uint32_t n;
+    uint32_t bucket;
+    uint32_t max_depth;     // min(cfg.max_depth, 16)
+    uint32_t first_tile;    // first radix tile of this simulation
+    uint32_t flags;         // BH_FLAG_*
+    double theta;
+    float theta_f;
+    float inv_theta_f;
+    float eps_f;            // softening as f32 (the reference squares the f32 value)
+    float g_f;
+    float dt;
+    float reserved;
+};
+
+// Per-simulation results of the last rebuild.
+struct SimOut {
+    double cx, cy, half;  // f64 root bounds (nbody/src/lib.rs:137-154)
+    double reserved;
+};
+
+struct Tile {
+    uint32_t sim;
+    uint32_t start;  // first position
+    uint32_t count;  // keys in this tile (<= kTile)
+    uint32_t reserved;
+};
+
+// Device buffers of one batch (all sized from the batch layout).
+struct BatchBuffers {
+    const SimDesc* sims;
+    SimOut* simout;
+    const uint32_t* chunk_sim;  // P/32 entries, kNone for unused chunks
+    const Tile* tiles;
+    uint32_t nsims;
+    uint32_t npos;     // P, multiple of 32
+    uint32_t nchunks;  // P / 32
+    uint32_t ntiles;
+    uint32_t nscan_tiles;
+    uint32_t cell_capacity;
+    // zeroed once per rebuild (one memset): control block
+    uint32_t* minmax;      // nsims * 4 (atomicMax of encoded floats; mins stored inverted)
+    uint32_t* hist;        // nsims * 4 * 256
+    uint32_t* counters;    // 8: radix tile counters (4), scan tile counter
+    uint32_t* sort_flags;  // 4 * ntiles * 256
+    unsigned long long* scan_flags;  // nscan_tiles
+    // transient per rebuild
+    uint32_t* keys_a;
+    uint32_t* keys_b;
+    uint32_t* vals_a;
+    uint32_t* vals_b;
+    float4* sbody;      // sorted (x, y, m, body index bits)
+    uint32_t* base;     // npos + 1: first cell index of each position's chain
+    float4* cell_f;     // com_x, com_y, mass, width (f32)
+    uint4* cell_u;      // start, end, skip, depth (global positions)
+    double4* cell_d;    // com_x, com_y, mass, 0 (f64)
+    uint4* cell_child;  // children (global cell indices)
+    uint32_t* cell_parent;
+    uint32_t* cell_counter;
+    // persistent
+    uint32_t* err;                   // error bits
+    unsigned long long* force_stats; // 4 counters
+};
+
+// ---- launchers (bh_kernels.cu) -------------------------------------------
+// mode: 0 bounds only, 1 kick_drift (+bounds), 2 final_kick, 3 final_kick+kick_drift (+bounds)
+cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s);
+cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s);
+cudaError_t launch_radix(const BatchBuffers& b, cudaStream_t s);
+cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s);
+cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s);
+cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s);
+cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
+                            cudaStream_t s);
+cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,
+                          GpuCell* cells, cudaStream_t s);
+cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bodies,
+                                   const GpuEntry* entries, const GpuCell* cells, uint32_t n,
+                                   uint32_t ncells, float4* accel, uint32_t* err,
+                                   cudaStream_t s);
+// FP64 conservation partial sums: out gets 9 doubles (see galaxy_bh_conservation).
+cudaError_t launch_conservation(const GpuEvolveState* state, const float* potential, uint32_t n,
+                                double* partials, uint32_t nblocks, double* out,
+                                cudaStream_t s);
+uint32_t conservation_blocks(uint32_t n);
+
+}  // namespace gbh

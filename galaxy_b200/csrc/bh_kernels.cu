@@ -1,0 +1,1241 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// sm_100a kernels of the Barnes-Hut evolution step.  Every kernel covers all
+// simulations of a batch in one launch (the plain path is a batch of one):
+//
+//   k_integrate   kick/drift/final-kick (runtime/src/nbody_evolve.wgsl) fused
+//                 with the per-simulation f32 min/max bounds reduction
+//   k_morton      f64 root bounds + 16-bit/axis quantization + Morton code
+//                 (nbody/src/lib.rs:137-154, nbody/src/flat.rs:67-94), fused
+//                 with the four 8-bit digit histograms of the radix sort
+//   k_radix_pass  one stable LSD pass (onesweep: decoupled look-back, warp
+//                 match ranking, shared-memory staged scatter); the last pass
+//                 also gathers the bodies into Morton order
+//   k_count_scan  cells per position + exclusive scan (cell numbering in the
+//                 reference's recursive preorder, nbody/src/flat.rs:127-177)
+//   k_cells       ranges, children, skip pointers of every cell
+//   k_aggregate   bottom-up f64 mass / centre of mass, identical arithmetic
+//                 and order to nbody/src/flat.rs:179-215
+//   k_traverse    warp-cooperative theta-MAC traversal (nbody/src/flat.rs:
+//                 270-346 per body), f32 forces, exact f64 MAC in the guard band
+//
+// The f64 expressions that must reproduce the reference bit for bit use the
+// explicit round-to-nearest intrinsics (__dadd_rn, __dmul_rn, ...), which
+// nvcc never contracts into FMAs.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "bh_internal.cuh"
+
+namespace gbh {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ void set_err(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
+
+// Order-preserving float <-> uint mapping (for integer atomics on floats).
+__device__ __forceinline__ uint32_t enc_f32(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float dec_f32(uint32_t e) {
+    uint32_t u = (e & 0x80000000u) ? (e & 0x7fffffffu) : ~e;
+    return __uint_as_float(u);
+}
+
+struct RootBounds {
+    double cx, cy, half;
+};
+
+// nbody/src/lib.rs:137-154 over the f32 min/max promoted to f64.
+__device__ __forceinline__ RootBounds root_bounds_from(const uint32_t* mm) {
+    double min_x = (double)dec_f32(~mm[0]);
+    double min_y = (double)dec_f32(~mm[1]);
+    double max_x = (double)dec_f32(mm[2]);
+    double max_y = (double)dec_f32(mm[3]);
+    double span = fmax(fmax(__dsub_rn(max_x, min_x), __dsub_rn(max_y, min_y)), 1e-12);
+    RootBounds r;
+    r.cx = __dmul_rn(__dadd_rn(min_x, max_x), 0.5);
+    r.cy = __dmul_rn(__dadd_rn(min_y, max_y), 0.5);
+    r.half = __dadd_rn(__dmul_rn(span, 0.500000000001), 1e-12);
+    return r;
+}
+
+// nbody/src/flat.rs:82-87
+__device__ __forceinline__ uint32_t quantize_axis(double value, double center, double half) {
+    double low = __dsub_rn(center, half);
+    double width = __dmul_rn(half, 2.0);
+    double scaled = floor(__dmul_rn(__ddiv_rn(__dsub_rn(value, low), width), 65536.0));
+    scaled = fmin(fmax(scaled, 0.0), 65535.0);
+    return (uint32_t)scaled;
+}
+
+// nbody/src/flat.rs:67-80
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {
+    v &= 0x0000ffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+__device__ __forceinline__ uint32_t morton2(uint32_t x, uint32_t y) {
+    return spread16(x) | (spread16(y) << 1);
+}
+
+// Number of leading quadtree levels (2 bits each) two codes share; 16 when equal.
+__device__ __forceinline__ uint32_t shared_levels(uint32_t a, uint32_t b) {
+    return a == b ? 16u : ((uint32_t)__clz(a ^ b) >> 1);
+}
+
+// 2^-d as an exact double.
+__device__ __forceinline__ double pow2_neg(uint32_t d) {
+    return __longlong_as_double((long long)(1023 - (int)d) << 52);
+}
+
+// First index in [lo, hi) whose code is >= x, given codes[j] < x for j < lo.
+// Exponential probe from lo, then binary search: O(log distance).
+__device__ __forceinline__ uint32_t gallop_lower_bound(const uint32_t* codes, uint32_t lo,
+                                                       uint32_t hi, uint32_t x) {
+    uint32_t step = 1;
+    uint32_t probe = lo;
+    while (probe < hi && codes[probe] < x) {
+        lo = probe + 1;
+        probe = lo + step;
+        step <<= 1;
+    }
+    uint32_t r = probe < hi ? probe : hi;
+    while (lo < r) {
+        uint32_t m = lo + ((r - lo) >> 1);
+        if (codes[m] < x)
+            lo = m + 1;
+        else
+            r = m;
+    }
+    return lo;
+}
+
+// Exclusive scan over a 256-thread block; *total gets the block sum.
+__device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* total,
+                                                             uint32_t* smem8) {
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(kFull, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    if (lane == 31) smem8[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < 8 ? smem8[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            uint32_t y = __shfl_up_sync(kFull, w, o);
+            if (lane >= (uint32_t)o) w += y;
+        }
+        if (lane < 8) smem8[lane] = w;
+    }
+    __syncthreads();
+    uint32_t wp = warp ? smem8[warp - 1] : 0u;
+    *total = smem8[7];
+    __syncthreads();
+    return wp + x - v;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) {
+    return *(const volatile uint32_t*)p;
+}
+__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long* p) {
+    return *(const volatile unsigned long long*)p;
+}
+
+// Bounded wait budget for look-back spins (~1 s at 2 GHz).
+constexpr long long kSpinCycles = 2000000000ll;
+
+}  // namespace
+
+// ============================================================ integrate ====
+
+// runtime/src/nbody_evolve.wgsl:19-46 with explicit f32 roundings (no FMA):
+// half_velocity = v + (0.5*dt)*a ; x = x + dt*half_velocity.  Mode 3 runs the
+// final kick of one step and the kick-drift of the next with the same two
+// roundings as two separate launches.  Modes 0, 1, 3 also reduce the
+// per-simulation f32 bounds of the (new) positions.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ sims,
+                                                   const uint32_t* __restrict__ chunk_sim,
+                                                   uint32_t nchunks, uint32_t* minmax) {
+    constexpr bool kBounds = MODE != 2;
+    __shared__ uint32_t s_sim[8];
+    __shared__ float s_val[8][4];
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * 8;
+    uint32_t cur = kNone;
+    float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
+
+    auto warp_reduce = [&]() {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(kFull, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(kFull, mny, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(kFull, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(kFull, mxy, o));
+        }
+    };
+
+    for (uint32_t chunk = blockIdx.x * 8 + warp; chunk < nchunks; chunk += nwarps) {
+        const uint32_t s = chunk_sim[chunk];
+        if (s == kNone) continue;
+        if (kBounds && s != cur) {
+            if (cur != kNone) {
+                warp_reduce();
+                if (lane == 0) {
+                    atomicMax(&minmax[4 * cur + 0], ~enc_f32(mnx));
+                    atomicMax(&minmax[4 * cur + 1], ~enc_f32(mny));
+                    atomicMax(&minmax[4 * cur + 2], enc_f32(mxx));
+                    atomicMax(&minmax[4 * cur + 3], enc_f32(mxy));
+                }
+                mnx = mny = INFINITY;
+                mxx = mxy = -INFINITY;
+            }
+            cur = s;
+        }
+        const SimDesc& sd = sims[s];
+        const uint32_t i = chunk * kChunk + lane - sd.off;
+        if (i < sd.n) {
+            float4* rec = reinterpret_cast<float4*>(sd.state + i);
+            float4 pm = rec[0];
+            if (MODE != 0) {
+                float4 v = rec[1];
+                const float4 a = sd.accel[i];
+                const float dt = sd.dt;
+                const float hdt = __fmul_rn(0.5f, dt);
+                if (MODE == 2 || MODE == 3) {
+                    v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
+                    v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
+                }
+                if (MODE == 1 || MODE == 3) {
+                    v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
+                    v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
+                    pm.x = __fadd_rn(pm.x, __fmul_rn(dt, v.x));
+                    pm.y = __fadd_rn(pm.y, __fmul_rn(dt, v.y));
+                    rec[0] = pm;
+                }
+                rec[1] = v;
+            }
+            if (kBounds) {
+                mnx = fminf(mnx, pm.x);
+                mny = fminf(mny, pm.y);
+                mxx = fmaxf(mxx, pm.x);
+                mxy = fmaxf(mxy, pm.y);
+            }
+        }
+    }
+    if (!kBounds) return;
+    warp_reduce();
+    if (lane == 0) {
+        s_sim[warp] = cur;
+        s_val[warp][0] = mnx;
+        s_val[warp][1] = mny;
+        s_val[warp][2] = mxx;
+        s_val[warp][3] = mxy;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = kNone;
+        float a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int w = 0; w <= 8; ++w) {
+            const uint32_t sw = w < 8 ? s_sim[w] : kNone;
+            if (w == 8 || sw != run) {
+                if (run != kNone) {
+                    atomicMax(&minmax[4 * run + 0], ~enc_f32(a0));
+                    atomicMax(&minmax[4 * run + 1], ~enc_f32(a1));
+                    atomicMax(&minmax[4 * run + 2], enc_f32(a2));
+                    atomicMax(&minmax[4 * run + 3], enc_f32(a3));
+                }
+                if (w == 8) break;
+                run = sw;
+                a0 = s_val[w][0];
+                a1 = s_val[w][1];
+                a2 = s_val[w][2];
+                a3 = s_val[w][3];
+            } else {
+                a0 = fminf(a0, s_val[w][0]);
+                a1 = fminf(a1, s_val[w][1]);
+                a2 = fmaxf(a2, s_val[w][2]);
+                a3 = fmaxf(a3, s_val[w][3]);
+            }
+        }
+    }
+}
+
+// ============================================================== morton ====
+
+// One block per radix tile: Morton codes of the tile's bodies (resident
+// order) plus the tile's contribution to the four digit histograms.
+__global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restrict__ sims,
+                                                         const Tile* __restrict__ tiles,
+                                                         const uint32_t* __restrict__ minmax,
+                                                         uint32_t* __restrict__ keys,
+                                                         uint32_t* hist, SimOut* simout) {
+    __shared__ uint32_t sh[kRadixPasses][kRadixDigits];
+    for (int k = threadIdx.x; k < kRadixPasses * kRadixDigits; k += kSortThreads)
+        (&sh[0][0])[k] = 0;
+    __syncthreads();
+    const Tile t = tiles[blockIdx.x];
+    const SimDesc& sd = sims[t.sim];
+    const RootBounds rb = root_bounds_from(minmax + 4 * t.sim);
+    if (threadIdx.x == 0 && t.start == sd.off) {
+        simout[t.sim].cx = rb.cx;
+        simout[t.sim].cy = rb.cy;
+        simout[t.sim].half = rb.half;
+    }
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const uint32_t idx = k * kSortThreads + threadIdx.x;
+        if (idx < t.count) {
+            const uint32_t p = t.start + idx;
+            const float2 xy = *reinterpret_cast<const float2*>(sd.state + (p - sd.off));
+            const uint32_t code = morton2(quantize_axis((double)xy.x, rb.cx, rb.half),
+                                          quantize_axis((double)xy.y, rb.cy, rb.half));
+            keys[p] = code;
+#pragma unroll
+            for (int pass = 0; pass < kRadixPasses; ++pass)
+                atomicAdd(&sh[pass][(code >> (8 * pass)) & 255u], 1u);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kRadixPasses * kRadixDigits; k += kSortThreads) {
+        const uint32_t c = (&sh[0][0])[k];
+        if (c) atomicAdd(&hist[(size_t)t.sim * kRadixPasses * kRadixDigits + k], c);
+    }
+}
+
+// ============================================================== radix =====
+
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kFlagMask = (1u << 30) - 1u;
+
+// One stable 8-bit LSD pass over every simulation's keys.  Tiles never cross
+// simulations; within a simulation, tile order is key order and the
+// decoupled look-back adds the digit counts of the preceding tiles.  Items
+// are ranked warp by warp in key order (match_any peers), so equal digits keep
+// their input order: the permutation equals a stable sort by code, as
+// Rust's sort_by_key (nbody/src/flat.rs:233-234).
+template <int PASS, bool LAST>
+__global__ void __launch_bounds__(kSortThreads) k_radix_pass(
+    const SimDesc* __restrict__ sims, const Tile* __restrict__ tiles, uint32_t* tile_counter,
+    const uint32_t* __restrict__ hist, uint32_t* flags, const uint32_t* __restrict__ keys_in,
+    const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, float4* __restrict__ sbody, uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_whist[8][kRadixDigits];
+    __shared__ uint32_t s_tprefix[kRadixDigits];
+    __shared__ uint32_t s_out[kRadixDigits];
+    __shared__ uint32_t s_keys[kTile];
+    __shared__ uint32_t s_vals[kTile];
+    __shared__ uint32_t s_scan[8];
+
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    for (int k = threadIdx.x; k < 8 * kRadixDigits; k += kSortThreads) (&s_whist[0][0])[k] = 0;
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const Tile tl = tiles[t];
+    const SimDesc& sd = sims[tl.sim];
+    const uint32_t shift = 8u * PASS;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+
+    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t idx = warp * 256u + r * 32u + lane;
+        const bool valid = idx < tl.count;
+        const uint32_t p = tl.start + idx;
+        key[r] = valid ? keys_in[p] : 0u;
+        val[r] = valid ? (PASS == 0 ? p - sd.off : vals_in[p]) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t idx = warp * 256u + r * 32u + lane;
+        const bool valid = idx < tl.count;
+        const uint32_t d = valid ? ((key[r] >> shift) & 255u) : (256u + lane);
+        const uint32_t peers = __match_any_sync(kFull, d);
+        const uint32_t leader = __ffs(peers) - 1u;
+        uint32_t b = 0;
+        if (valid && lane == leader) {
+            b = s_whist[warp][d];
+            s_whist[warp][d] = b + __popc(peers);
+        }
+        b = __shfl_sync(kFull, b, leader);
+        rank[r] = b + __popc(peers & lt_mask);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Thread d owns digit d: warp offsets, tile count, look-back, bases.
+    const uint32_t d = threadIdx.x;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const uint32_t c = s_whist[w][d];
+        s_whist[w][d] = run;
+        run += c;
+    }
+    const bool first = (t == sd.first_tile);
+    uint32_t* my_flag = flags + (size_t)t * kRadixDigits + d;
+    atomicExch(my_flag, (first ? kFlagInc : kFlagAgg) | run);
+    uint32_t excl = 0;
+    if (!first) {
+        uint32_t tp = t - 1;
+        const long long t0 = clock64();
+        while (true) {
+            const uint32_t f = ld_volatile(flags + (size_t)tp * kRadixDigits + d);
+            const uint32_t st = f & ~kFlagMask;
+            if (st == 0u) {
+                if (clock64() - t0 > kSpinCycles) {
+                    set_err(err, kErrLookbackTimeout);
+                    break;
+                }
+                continue;
+            }
+            excl += f & kFlagMask;
+            if (st == kFlagInc) break;
+            --tp;
+        }
+        atomicExch(my_flag, kFlagInc | (excl + run));
+    }
+    uint32_t tot;
+    const uint32_t h = hist[((size_t)tl.sim * kRadixPasses + PASS) * kRadixDigits + d];
+    const uint32_t gex = block_exclusive_scan_256(h, &tot, s_scan);
+    const uint32_t tex = block_exclusive_scan_256(run, &tot, s_scan);
+    s_tprefix[d] = tex;
+    s_out[d] = sd.off + gex + excl - tex;
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t idx = warp * 256u + r * 32u + lane;
+        if (idx < tl.count) {
+            const uint32_t dg = (key[r] >> shift) & 255u;
+            const uint32_t slot = s_tprefix[dg] + s_whist[warp][dg] + rank[r];
+            s_keys[slot] = key[r];
+            s_vals[slot] = val[r];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortItems; ++k) {
+        const uint32_t slot = k * kSortThreads + threadIdx.x;
+        if (slot < tl.count) {
+            const uint32_t kk = s_keys[slot];
+            const uint32_t vv = s_vals[slot];
+            const uint32_t dest = s_out[(kk >> shift) & 255u] + slot;
+            keys_out[dest] = kk;
+            vals_out[dest] = vv;
+            if (LAST) {
+                const float4 pm = *reinterpret_cast<const float4*>(sd.state + vv);
+                sbody[dest] = make_float4(pm.x, pm.y, pm.z, __uint_as_float(vv));
+            }
+        }
+    }
+}
+
+// ========================================================== count + scan ==
+
+// Cells whose range starts at sorted position i (a "chain": depths
+// d_min..D).  Cell (d, i) exists iff i starts a depth-d group and its parent
+// group holds more than `bucket` bodies; it is internal iff it holds more
+// than `bucket` bodies and d < max_depth (nbody/src/flat.rs:145).
+__device__ __forceinline__ uint32_t chain_count(const uint32_t* __restrict__ sc, uint32_t i,
+                                                uint32_t n, uint32_t bucket, uint32_t maxd,
+                                                uint32_t* dmin_out) {
+    const uint32_t ci = sc[i];
+    const uint32_t dmin = i == 0 ? 0u : shared_levels(sc[i - 1], ci) + 1u;
+    *dmin_out = dmin;
+    if (dmin > maxd) return 0;
+    if (i > 0 && bucket > 1) {
+        // parent group (depth dmin-1) holds i-1 and i; needs > bucket bodies:
+        // some window [j, j+bucket] containing both lies inside it.
+        const uint32_t pd = dmin - 1u;
+        const uint32_t jlo = i >= bucket ? i - bucket : 0u;
+        bool ok = false;
+        for (uint32_t j = jlo; j < i && j + bucket < n; ++j) {
+            if (shared_levels(sc[j], sc[j + bucket]) >= pd) {
+                ok = true;
+                break;
+            }
+        }
+        if (!ok) return 0;
+    }
+    const int lw = (i + bucket < n) ? (int)shared_levels(ci, sc[i + bucket]) : -1;
+    const int deepest = max((int)dmin, min((int)maxd, lw + 1));
+    return (uint32_t)(deepest - (int)dmin + 1);
+}
+
+constexpr unsigned long long kScanAgg = 1ull << 62;
+constexpr unsigned long long kScanInc = 2ull << 62;
+constexpr unsigned long long kScanMask = (1ull << 62) - 1ull;
+
+__global__ void __launch_bounds__(kScanThreads) k_count_scan(
+    const SimDesc* __restrict__ sims, const uint32_t* __restrict__ chunk_sim, uint32_t npos,
+    const uint32_t* __restrict__ codes, uint32_t* __restrict__ base, uint32_t* tile_counter,
+    unsigned long long* flags, uint32_t* err) {
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[8];
+    __shared__ unsigned long long s_excl;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const uint32_t p0 = t * kScanTile + threadIdx.x * kScanItems;
+    uint32_t cnt[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t p = p0 + k;
+        uint32_t c = 0;
+        if (p < npos) {
+            const uint32_t s = chunk_sim[p >> 5];
+            if (s != kNone) {
+                const SimDesc& sd = sims[s];
+                const uint32_t i = p - sd.off;
+                if (i < sd.n) {
+                    uint32_t dmin;
+                    c = chain_count(codes + sd.off, i, sd.n, sd.bucket, sd.max_depth, &dmin);
+                }
+            }
+        }
+        cnt[k] = c;
+        sum += c;
+    }
+    uint32_t tile_total;
+    const uint32_t texcl = block_exclusive_scan_256(sum, &tile_total, s_scan);
+    if (threadIdx.x == 0) {
+        unsigned long long excl = 0;
+        if (t == 0) {
+            atomicExch(&flags[0], kScanInc | (unsigned long long)tile_total);
+        } else {
+            atomicExch(&flags[t], kScanAgg | (unsigned long long)tile_total);
+            uint32_t tp = t - 1;
+            const long long c0 = clock64();
+            while (true) {
+                const unsigned long long f = ld_volatile64(&flags[tp]);
+                const unsigned long long st = f & ~kScanMask;
+                if (st == 0ull) {
+                    if (clock64() - c0 > kSpinCycles) {
+                        set_err(err, kErrLookbackTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                excl += f & kScanMask;
+                if (st == kScanInc) break;
+                --tp;
+            }
+            atomicExch(&flags[t], kScanInc | (excl + tile_total));
+        }
+        s_excl = excl;
+    }
+    __syncthreads();
+    uint32_t run = (uint32_t)s_excl + texcl;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t p = p0 + k;
+        if (p <= npos) base[p] = run;
+        run += cnt[k];
+    }
+}
+
+// =============================================================== cells ====
+
+// End (exclusive, sim-local) of the depth-d group containing sorted position
+// i, searching from `from`.
+__device__ __forceinline__ uint32_t group_end(const uint32_t* __restrict__ sc, uint32_t n,
+                                              uint32_t i, uint32_t d, uint32_t from) {
+    if (d == 0) return n;
+    const uint32_t sh = 32u - 2u * d;
+    const unsigned long long next = ((unsigned long long)(sc[i] >> sh) + 1ull) << sh;
+    if (next > 0xffffffffull) return n;
+    return gallop_lower_bound(sc, from, n, (uint32_t)next);
+}
+
+__global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
+                                               const uint32_t* __restrict__ chunk_sim,
+                                               uint32_t npos, uint32_t capacity,
+                                               const uint32_t* __restrict__ codes,
+                                               const uint32_t* __restrict__ base, uint4* cell_u,
+                                               uint4* cell_child, uint32_t* cell_parent,
+                                               uint32_t* cell_counter, uint32_t* err) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npos) return;
+    const uint32_t s = chunk_sim[p >> 5];
+    if (s == kNone) return;
+    const SimDesc& sd = sims[s];
+    const uint32_t i = p - sd.off;
+    if (i >= sd.n) return;
+    const uint32_t k0 = base[p];
+    const uint32_t c = base[p + 1] - k0;
+    if (c == 0) return;
+    if (k0 + c > capacity) {
+        set_err(err, kErrCapacity);
+        return;
+    }
+    const uint32_t* sc = codes + sd.off;
+    const uint32_t n = sd.n;
+    const uint32_t dmin = i == 0 ? 0u : shared_levels(sc[i - 1], sc[i]) + 1u;
+    const uint32_t deepest = dmin + c - 1u;
+    uint32_t ends[kMortonDepth + 1];
+    uint32_t from = i + 1;
+    for (int d = (int)deepest; d >= (int)dmin; --d) {
+        from = group_end(sc, n, i, (uint32_t)d, from);
+        ends[d - dmin] = from;
+    }
+    if (dmin == 0) cell_parent[k0] = kNone;
+    for (uint32_t d = dmin; d <= deepest; ++d) {
+        const uint32_t k = k0 + (d - dmin);
+        const uint32_t end = ends[d - dmin];
+        cell_u[k] = make_uint4(p, sd.off + end, base[sd.off + end], d);
+        cell_counter[k] = 0;
+        uint4 ch = make_uint4(kNone, kNone, kNone, kNone);
+        if (d < deepest) {
+            const uint32_t sh = 30u - 2u * d;
+            const uint32_t pre = d == 0 ? 0u : (sc[i] >> (32u - 2u * d));
+            uint32_t lo = i;
+            uint32_t bounds[5];
+            bounds[0] = i;
+#pragma unroll
+            for (uint32_t q = 1; q < 4; ++q) {
+                const uint32_t x = ((pre << 2) | q) << sh;
+                lo = gallop_lower_bound(sc, lo, end, x);
+                bounds[q] = lo;
+            }
+            bounds[4] = end;
+            uint32_t* chp = &ch.x;
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) {
+                if (bounds[q] < bounds[q + 1]) {
+                    const uint32_t child = bounds[q] == i ? k + 1u : base[sd.off + bounds[q]];
+                    chp[q] = child;
+                    if (child < capacity)
+                        cell_parent[child] = k;
+                    else
+                        set_err(err, kErrCapacity);
+                }
+            }
+        }
+        cell_child[k] = ch;
+    }
+}
+
+// =========================================================== aggregate ====
+
+__device__ __forceinline__ void store_cell_values(uint32_t k, double mass, double wx, double wy,
+                                                  uint32_t depth, double root_half,
+                                                  double4* cell_d, float4* cell_f) {
+    const double com_x = __ddiv_rn(wx, mass);
+    const double com_y = __ddiv_rn(wy, mass);
+    cell_d[k] = make_double4(com_x, com_y, mass, 0.0);
+    const double half = __dmul_rn(root_half, pow2_neg(depth));
+    cell_f[k] = make_float4((float)com_x, (float)com_y, (float)mass, (float)__dmul_rn(half, 2.0));
+}
+
+// Leaves (the last cell of each chain) sum their bodies in Morton order; the
+// last child to finish a parent sums the children in quadrant order
+// 0..3 — the arithmetic and order of nbody/src/flat.rs:179-215, so the f64
+// mass and centre of mass equal the reference's bit for bit.
+__global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ sims,
+                                                   const SimOut* __restrict__ simout,
+                                                   const uint32_t* __restrict__ chunk_sim,
+                                                   uint32_t npos, const uint32_t* __restrict__ base,
+                                                   const float4* __restrict__ sbody,
+                                                   const uint4* __restrict__ cell_u,
+                                                   const uint4* __restrict__ cell_child,
+                                                   const uint32_t* __restrict__ cell_parent,
+                                                   uint32_t* cell_counter, double4* cell_d,
+                                                   float4* cell_f) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npos) return;
+    const uint32_t s = chunk_sim[p >> 5];
+    if (s == kNone) return;
+    const SimDesc& sd = sims[s];
+    if (p - sd.off >= sd.n) return;
+    const uint32_t k0 = base[p];
+    const uint32_t c = base[p + 1] - k0;
+    if (c == 0) return;
+    const double root_half = simout[s].half;
+    uint32_t k = k0 + c - 1u;
+    {
+        const uint4 u = cell_u[k];
+        double mass = 0.0, wx = 0.0, wy = 0.0;
+        for (uint32_t q = u.x; q < u.y; ++q) {
+            const float4 b = sbody[q];
+            const double m = (double)b.z;
+            mass = __dadd_rn(mass, m);
+            wx = __dadd_rn(wx, __dmul_rn(m, (double)b.x));
+            wy = __dadd_rn(wy, __dmul_rn(m, (double)b.y));
+        }
+        store_cell_values(k, mass, wx, wy, u.w, root_half, cell_d, cell_f);
+    }
+    while (true) {
+        const uint32_t par = cell_parent[k];
+        if (par == kNone) break;
+        const uint4 ch = cell_child[par];
+        const uint32_t nchild = (ch.x != kNone) + (ch.y != kNone) + (ch.z != kNone) + (ch.w != kNone);
+        __threadfence();
+        const uint32_t old = atomicAdd(&cell_counter[par], 1u);
+        if (old + 1u != nchild) break;
+        __threadfence();
+        double mass = 0.0, wx = 0.0, wy = 0.0;
+        const uint32_t chv[4] = {ch.x, ch.y, ch.z, ch.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (chv[q] == kNone) continue;
+            const double2 cxy = __ldcg(reinterpret_cast<const double2*>(cell_d + chv[q]));
+            const double cm = __ldcg(reinterpret_cast<const double*>(cell_d + chv[q]) + 2);
+            mass = __dadd_rn(mass, cm);
+            wx = __dadd_rn(wx, __dmul_rn(cm, cxy.x));
+            wy = __dadd_rn(wy, __dmul_rn(cm, cxy.y));
+        }
+        store_cell_values(par, mass, wx, wy, cell_u[par].w, root_half, cell_d, cell_f);
+        k = par;
+    }
+}
+
+// ============================================================ traverse ====
+
+template <bool COMP>
+struct Acc {
+    float x = 0.f, y = 0.f, cx = 0.f, cy = 0.f;
+    __device__ __forceinline__ void add(float tx, float ty) {
+        if (COMP) {
+            // Knuth two-sum: s + e == x + tx exactly.
+            float s = x + tx;
+            float bb = s - x;
+            cx += (x - (s - bb)) + (tx - bb);
+            x = s;
+            s = y + ty;
+            bb = s - y;
+            cy += (y - (s - bb)) + (ty - bb);
+            y = s;
+        } else {
+            x += tx;
+            y += ty;
+        }
+    }
+    __device__ __forceinline__ float fx() const { return COMP ? x + cx : x; }
+    __device__ __forceinline__ float fy() const { return COMP ? y + cy : y; }
+};
+
+// Warp-cooperative traversal.  A warp owns 32 consecutive Morton positions
+// and walks the union of its lanes' traversals in preorder using skip
+// pointers (first child = next cell, skip = next cell after the subtree).
+// Each lane keeps exactly its own decisions: lane L acts on a cell only if
+// L opened the cell's parent (mask held per depth in lane `depth`), so every
+// lane visits the cells of nbody/src/flat.rs:270-346 in the same order and
+// sums the same terms in the same order.  The MAC is decided in f32 unless
+// the f32 margin is inside a guard band, where it is re-decided in f64 from
+// the f64 centre of mass exactly as the reference computes it.
+template <bool COMP, bool POT, bool STATS>
+__global__ void __launch_bounds__(256) k_traverse(
+    const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
+    const uint32_t* __restrict__ chunk_sim, uint32_t nchunks, const float4* __restrict__ sbody,
+    const float4* __restrict__ cell_f, const uint4* __restrict__ cell_u,
+    const double4* __restrict__ cell_d, const uint32_t* __restrict__ base,
+    unsigned long long* stats, uint32_t* err) {
+    const uint32_t lane = lane_id();
+    const uint32_t chunk = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (chunk >= nchunks) return;
+    const uint32_t s = chunk_sim[chunk];
+    if (s == kNone) return;
+    const SimDesc& sd = sims[s];
+    const uint32_t p = chunk * kChunk + lane;
+    const uint32_t end_pos = sd.off + sd.n;
+    const bool valid = p < end_pos;
+    const float4 me = valid ? sbody[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float tx = me.x, ty = me.y;
+    const float eps2 = sd.eps_f * sd.eps_f;
+    const float g = sd.g_f;
+    const float inv_theta = sd.inv_theta_f;
+    const double theta = sd.theta;
+    const double root_half = simout[s].half;
+    const uint32_t valid_mask = __ballot_sync(kFull, valid);
+    uint32_t c = base[sd.off];
+    const uint32_t cend = base[end_pos];
+    uint32_t om = 0;  // lane d: mask of lanes that opened the current depth-d ancestor
+    Acc<COMP> acc;
+    float phi = 0.f;
+    uint32_t n_visit = 0, n_approx = 0, n_direct = 0, n_exact = 0;
+
+    auto interact = [&](float dx, float dy, float m) {
+        const float r2 = dx * dx + dy * dy + eps2;
+        const float inv_r = rsqrtf(r2);
+        const float scale = g * m * inv_r * inv_r * inv_r;
+        acc.add(dx * scale, dy * scale);
+        if (POT) phi -= g * m * inv_r;
+    };
+
+    while (c < cend) {
+        const uint4 u = cell_u[c];
+        const float4 f = cell_f[c];
+        const uint32_t depth = u.w;
+        const uint32_t M = depth == 0 ? valid_mask : __shfl_sync(kFull, om, (depth - 1u) & 31u);
+        const bool active = (M >> lane) & 1u;
+        if (STATS && active) ++n_visit;
+        if (u.z <= c) {
+            set_err(err, kErrTraversal);
+            break;
+        }
+        if (u.z == c + 1u) {
+            // leaf: always summed directly (flat.rs:297-315), self excluded
+            if (u.y - u.x == 1u) {
+                if (active && u.x != p) {
+                    interact(f.x - tx, f.y - ty, f.z);
+                    if (STATS) ++n_direct;
+                }
+            } else {
+                for (uint32_t q = u.x; q < u.y; ++q) {
+                    const float4 b = sbody[q];
+                    if (active && q != p) {
+                        interact(b.x - tx, b.y - ty, b.z);
+                        if (STATS) ++n_direct;
+                    }
+                }
+            }
+            c = u.z;
+            continue;
+        }
+        bool open = false;
+        if (active) {
+            const bool contains = p >= u.x && p < u.y;
+            const float dx = f.x - tx, dy = f.y - ty;
+            if (contains || !(theta > 0.0)) {
+                open = true;
+            } else {
+                const float d2 = dx * dx + dy * dy;
+                const float crit = f.w * inv_theta;
+                const float crit2 = crit * crit;
+                const float a = 2.4e-7f * (fabsf(f.x) + fabsf(f.y) + fabsf(dx) + fabsf(dy));
+                const float guard = 1e-4f * crit2 + 4.f * crit * a + 4.f * a * a;
+                const float margin = d2 - crit2;
+                bool approx;
+                if (margin > guard) {
+                    approx = true;
+                } else if (margin < -guard) {
+                    approx = false;
+                } else {
+                    // f64 MAC exactly as flat.rs:317-323
+                    const double2 com = *reinterpret_cast<const double2*>(cell_d + c);
+                    const double ddx = __dsub_rn(com.x, (double)tx);
+                    const double ddy = __dsub_rn(com.y, (double)ty);
+                    const double dist = hypot(ddx, ddy);
+                    const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(depth)), 2.0);
+                    approx = dist > 0.0 && __ddiv_rn(width, dist) < theta;
+                    if (STATS) ++n_exact;
+                }
+                if (approx) {
+                    interact(dx, dy, f.z);
+                    if (STATS) ++n_approx;
+                } else {
+                    open = true;
+                }
+            }
+        }
+        const uint32_t O = __ballot_sync(kFull, open);
+        if (O) {
+            if (lane == depth) om = O;
+            c = c + 1u;
+        } else {
+            c = u.z;
+        }
+    }
+    if (valid) {
+        const uint32_t idx = __float_as_uint(me.w);
+        sd.accel[idx] = make_float4(acc.fx(), acc.fy(), 0.f, 0.f);
+        if (POT && sd.potential) sd.potential[idx] = phi;
+    }
+    if (STATS) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            n_visit += __shfl_xor_sync(kFull, n_visit, o);
+            n_approx += __shfl_xor_sync(kFull, n_approx, o);
+            n_direct += __shfl_xor_sync(kFull, n_direct, o);
+            n_exact += __shfl_xor_sync(kFull, n_exact, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&stats[0], (unsigned long long)n_visit);
+            atomicAdd(&stats[1], (unsigned long long)n_approx);
+            atomicAdd(&stats[2], (unsigned long long)n_direct);
+            atomicAdd(&stats[3], (unsigned long long)n_exact);
+        }
+    }
+}
+
+// ======================================================== packed (2B1) ====
+
+// runtime/src/nbody.wgsl:43-123 (and barnes_hut_flat.cu:65-146) over an
+// arbitrary packed tree with explicit children: the same per-body decisions
+// (f32 MAC with sqrt) and order, computed warp-cooperatively over 32
+// consecutive Morton positions with a shared (cell, lane mask) stack.
+constexpr int kPackedStack = 64;
+
+__device__ __forceinline__ void packed_point_mass(float tx, float ty, float px, float py,
+                                                  float mass, float soft, float g, float* ax,
+                                                  float* ay) {
+    const float dx = px - tx;
+    const float dy = py - ty;
+    const float r2 = dx * dx + dy * dy + soft * soft;
+    const float inv_r = rsqrtf(r2);
+    const float scale = g * mass * inv_r * inv_r * inv_r;
+    *ax += dx * scale;
+    *ay += dy * scale;
+}
+
+__global__ void __launch_bounds__(256) k_traverse_packed(
+    const BhSettings* __restrict__ settings, const GpuBody* __restrict__ bodies,
+    const GpuEntry* __restrict__ entries, const GpuCell* __restrict__ cells, uint32_t n,
+    uint32_t ncells, float4* __restrict__ accel, uint32_t* err) {
+    __shared__ uint32_t s_cell[8][kPackedStack];
+    __shared__ uint32_t s_mask[8][kPackedStack];
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint32_t p = (blockIdx.x * 8 + warp) * 32u + lane;
+    if ((blockIdx.x * 8 + warp) * 32u >= n) return;
+    const BhSettings st = *settings;
+    const float theta = st.physics[0], soft = st.physics[1], g = st.physics[2];
+    const bool valid = p < n;
+    const uint32_t ti = valid ? entries[p].data[1] : 0u;
+    const bool ti_ok = ti < n;
+    const GpuBody tb = (valid && ti_ok) ? bodies[ti] : GpuBody{};
+    const float tx = tb.position_mass[0], ty = tb.position_mass[1];
+    const uint32_t tpos = tb.meta[0];
+    float ax = 0.f, ay = 0.f;
+    int len = 1;
+    const uint32_t vmask = __ballot_sync(kFull, valid && ti_ok);
+    if (lane == 0) {
+        s_cell[warp][0] = st.info[2];
+        s_mask[warp][0] = vmask;
+    }
+    __syncwarp();
+    while (len > 0) {
+        --len;
+        const uint32_t ci = s_cell[warp][len];
+        const uint32_t M = s_mask[warp][len];
+        __syncwarp();
+        if (ci >= ncells) {
+            set_err(err, kErrPackedIndex);
+            break;
+        }
+        const GpuCell cell = cells[ci];
+        const bool active = (M >> lane) & 1u;
+        const bool leaf = cell.children[0] == GALAXY_BH_NO_CHILD &&
+                          cell.children[1] == GALAXY_BH_NO_CHILD &&
+                          cell.children[2] == GALAXY_BH_NO_CHILD &&
+                          cell.children[3] == GALAXY_BH_NO_CHILD;
+        if (leaf) {
+            for (uint32_t q = cell.range_depth[0]; q < cell.range_depth[1]; ++q) {
+                if (q >= n) {
+                    set_err(err, kErrPackedIndex);
+                    break;
+                }
+                const uint32_t o = entries[q].data[1];
+                if (active && o != ti && o < n) {
+                    const GpuBody ob = bodies[o];
+                    packed_point_mass(tx, ty, ob.position_mass[0], ob.position_mass[1],
+                                      ob.position_mass[2], soft, g, &ax, &ay);
+                }
+            }
+            continue;
+        }
+        bool open = false;
+        if (active) {
+            const float dx = cell.com[0] - tx;
+            const float dy = cell.com[1] - ty;
+            const float distance2 = dx * dx + dy * dy;
+            const bool contains = tpos >= cell.range_depth[0] && tpos < cell.range_depth[1];
+            open = true;
+            if (!contains && distance2 > 0.0f) {
+                const float distance = sqrtf(distance2);
+                if ((2.0f * cell.center_half_mass[2]) / distance < theta) {
+                    packed_point_mass(tx, ty, cell.com[0], cell.com[1], cell.center_half_mass[3],
+                                      soft, g, &ax, &ay);
+                    open = false;
+                }
+            }
+        }
+        const uint32_t O = __ballot_sync(kFull, open);
+        if (O) {
+            int nch = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) nch += cell.children[q] != GALAXY_BH_NO_CHILD;
+            if (len + nch > kPackedStack) {
+                set_err(err, kErrPackedStack);
+                break;
+            }
+            if (lane == 0) {
+                for (int q = 3; q >= 0; --q) {
+                    if (cell.children[q] != GALAXY_BH_NO_CHILD) {
+                        s_cell[warp][len] = cell.children[q];
+                        s_mask[warp][len] = O;
+                        ++len;
+                    }
+                }
+            }
+            len = __shfl_sync(kFull, len, 0);
+            __syncwarp();
+        }
+    }
+    if (valid && ti_ok) accel[ti] = make_float4(ax, ay, 0.f, 0.f);
+}
+
+// ============================================================ export =====
+
+// Frozen 64-byte cells (pack_flat_tree, nbody_gpu.rs:211-229) of one
+// simulation in the reference preorder, plus sorted entries and bodies with
+// their Morton positions.  Cell centres are rebuilt from the code prefix
+// with the same f64 steps as child_bounds (nbody/src/flat.rs:96-103).
+__global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
+                               uint32_t sim, const uint32_t* __restrict__ codes,
+                               const uint32_t* __restrict__ base, const uint4* __restrict__ cell_u,
+                               const uint4* __restrict__ cell_child,
+                               const double4* __restrict__ cell_d, GpuCell* out) {
+    const SimDesc& sd = sims[sim];
+    const uint32_t cb = base[sd.off], ce = base[sd.off + sd.n];
+    const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ce) return;
+    const SimOut so = simout[sim];
+    const uint4 u = cell_u[k];
+    const uint32_t start = u.x - sd.off;
+    const uint32_t code = codes[u.x];
+    double cx = so.cx, cy = so.cy, half = so.half;
+    for (uint32_t level = 0; level < u.w; ++level) {
+        const uint32_t q = (code >> (30u - 2u * level)) & 3u;
+        const double h = __dmul_rn(half, 0.5);
+        cx = __dadd_rn(cx, (q & 1u) ? h : -h);
+        cy = __dadd_rn(cy, (q & 2u) ? h : -h);
+        half = h;
+    }
+    const double4 v = cell_d[k];
+    const uint4 ch = cell_child[k];
+    GpuCell c;
+    c.center_half_mass[0] = (float)cx;
+    c.center_half_mass[1] = (float)cy;
+    c.center_half_mass[2] = (float)half;
+    c.center_half_mass[3] = (float)v.z;
+    c.com[0] = (float)v.x;
+    c.com[1] = (float)v.y;
+    c.com[2] = 0.f;
+    c.com[3] = 0.f;
+    c.range_depth[0] = start;
+    c.range_depth[1] = u.y - sd.off;
+    c.range_depth[2] = u.w;
+    c.range_depth[3] = 0u;
+    c.children[0] = ch.x == kNone ? kNone : ch.x - cb;
+    c.children[1] = ch.y == kNone ? kNone : ch.y - cb;
+    c.children[2] = ch.z == kNone ? kNone : ch.z - cb;
+    c.children[3] = ch.w == kNone ? kNone : ch.w - cb;
+    out[k - cb] = c;
+}
+
+__global__ void k_export_entries(const SimDesc* __restrict__ sims, uint32_t sim,
+                                 const uint32_t* __restrict__ codes,
+                                 const float4* __restrict__ sbody, GpuEntry* entries,
+                                 GpuBody* bodies) {
+    const SimDesc& sd = sims[sim];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= sd.n) return;
+    const float4 b = sbody[sd.off + i];
+    const uint32_t idx = __float_as_uint(b.w);
+    if (entries) {
+        GpuEntry e;
+        e.data[0] = codes[sd.off + i];
+        e.data[1] = idx;
+        e.data[2] = 0u;
+        e.data[3] = 0u;
+        entries[i] = e;
+    }
+    if (bodies) {
+        GpuBody gb;
+        gb.position_mass[0] = b.x;
+        gb.position_mass[1] = b.y;
+        gb.position_mass[2] = b.z;
+        gb.position_mass[3] = 0.f;
+        gb.meta[0] = i;
+        gb.meta[1] = gb.meta[2] = gb.meta[3] = 0u;
+        bodies[idx] = gb;
+    }
+}
+
+// ======================================================= conservation =====
+
+constexpr int kConsThreads = 256;
+constexpr int kConsTerms = 9;
+
+// Per-block f64 partial sums in a fixed order, then one block adds the
+// partials in block order: the result does not depend on scheduling.
+__global__ void __launch_bounds__(kConsThreads) k_conservation_partial(
+    const GpuEvolveState* __restrict__ state, const float* __restrict__ potential, uint32_t n,
+    double* partials) {
+    __shared__ double sh[kConsTerms][kConsThreads];
+    double t[kConsTerms] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = blockIdx.x * kConsThreads + threadIdx.x; i < n;
+         i += gridDim.x * kConsThreads) {
+        const GpuEvolveState s = state[i];
+        const double m = s.position_mass[2], x = s.position_mass[0], y = s.position_mass[1];
+        const double vx = s.velocity[0], vy = s.velocity[1];
+        t[0] += m;
+        t[1] += m * x;
+        t[2] += m * y;
+        t[3] += m * vx;
+        t[4] += m * vy;
+        t[5] += m * (x * vy - y * vx);
+        t[6] += 0.5 * m * (vx * vx + vy * vy);
+        if (potential) t[7] += 0.5 * m * (double)potential[i];
+        t[8] += m * hypot(vx, vy);
+    }
+#pragma unroll
+    for (int k = 0; k < kConsTerms; ++k) sh[k][threadIdx.x] = t[k];
+    __syncthreads();
+    for (int stride = kConsThreads / 2; stride > 0; stride >>= 1) {
+        if ((int)threadIdx.x < stride)
+#pragma unroll
+            for (int k = 0; k < kConsTerms; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + stride];
+        __syncthreads();
+    }
+    if (threadIdx.x < kConsTerms) partials[blockIdx.x * kConsTerms + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void k_conservation_final(const double* partials, uint32_t nblocks, double* out) {
+    if (threadIdx.x >= kConsTerms) return;
+    double acc = 0.0;
+    for (uint32_t b = 0; b < nblocks; ++b) acc += partials[b * kConsTerms + threadIdx.x];
+    out[threadIdx.x] = acc;
+}
+
+// ============================================================ launchers ===
+
+static uint32_t integrate_blocks(uint32_t nchunks) {
+    uint32_t blocks = (nchunks + 7) / 8;
+    const uint32_t cap = 148u * 8u;
+    return blocks < cap ? (blocks ? blocks : 1u) : cap;
+}
+
+cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s) {
+    const uint32_t blocks = integrate_blocks(b.nchunks);
+    switch (mode) {
+        case 0: k_integrate<0><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
+        case 1: k_integrate<1><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
+        case 2: k_integrate<2><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
+        default: k_integrate<3><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s) {
+    k_morton<<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a, b.hist,
+                                               b.simout);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_radix(const BatchBuffers& b, cudaStream_t s) {
+    const size_t fstride = (size_t)b.ntiles * kRadixDigits;
+    k_radix_pass<0, false><<<b.ntiles, kSortThreads, 0, s>>>(
+        b.sims, b.tiles, b.counters + 0, b.hist, b.sort_flags, b.keys_a, nullptr, b.keys_b,
+        b.vals_b, b.sbody, b.err);
+    k_radix_pass<1, false><<<b.ntiles, kSortThreads, 0, s>>>(
+        b.sims, b.tiles, b.counters + 1, b.hist, b.sort_flags + fstride, b.keys_b, b.vals_b,
+        b.keys_a, b.vals_a, b.sbody, b.err);
+    k_radix_pass<2, false><<<b.ntiles, kSortThreads, 0, s>>>(
+        b.sims, b.tiles, b.counters + 2, b.hist, b.sort_flags + 2 * fstride, b.keys_a, b.vals_a,
+        b.keys_b, b.vals_b, b.sbody, b.err);
+    k_radix_pass<3, true><<<b.ntiles, kSortThreads, 0, s>>>(
+        b.sims, b.tiles, b.counters + 3, b.hist, b.sort_flags + 3 * fstride, b.keys_b, b.vals_b,
+        b.keys_a, b.vals_a, b.sbody, b.err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
+    k_count_scan<<<b.nscan_tiles, kScanThreads, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.keys_a,
+                                                        b.base, b.counters + 4, b.scan_flags,
+                                                        b.err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
+    k_cells<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
+                                                 b.keys_a, b.base, b.cell_u, b.cell_child,
+                                                 b.cell_parent, b.cell_counter, b.err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
+    k_aggregate<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.npos,
+                                                     b.base, b.sbody, b.cell_u, b.cell_child,
+                                                     b.cell_parent, b.cell_counter, b.cell_d,
+                                                     b.cell_f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
+                            cudaStream_t s) {
+    const uint32_t blocks = (b.nchunks + 7) / 8;
+#define GBH_TRAVERSE(C, P, S)                                                                  \
+    k_traverse<C, P, S><<<blocks, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.nchunks,      \
+                                               b.sbody, b.cell_f, b.cell_u, b.cell_d, b.base, \
+                                               b.force_stats, b.err)
+    if (stats) {
+        if (compensated) {
+            if (potential) GBH_TRAVERSE(true, true, true); else GBH_TRAVERSE(true, false, true);
+        } else {
+            if (potential) GBH_TRAVERSE(false, true, true); else GBH_TRAVERSE(false, false, true);
+        }
+    } else {
+        if (compensated) {
+            if (potential) GBH_TRAVERSE(true, true, false); else GBH_TRAVERSE(true, false, false);
+        } else {
+            if (potential) GBH_TRAVERSE(false, true, false); else GBH_TRAVERSE(false, false, false);
+        }
+    }
+#undef GBH_TRAVERSE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,
+                          GpuCell* cells, cudaStream_t s) {
+    if (cells)
+        k_export_cells<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
+            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_u, b.cell_child, b.cell_d, cells);
+    if (entries || bodies)
+        k_export_entries<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, sim, b.keys_a, b.sbody,
+                                                             entries, bodies);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bodies,
+                                   const GpuEntry* entries, const GpuCell* cells, uint32_t n,
+                                   uint32_t ncells, float4* accel, uint32_t* err,
+                                   cudaStream_t s) {
+    const uint32_t warps = (n + 31) / 32;
+    k_traverse_packed<<<(warps + 7) / 8, 256, 0, s>>>(settings, bodies, entries, cells, n, ncells,
+                                                      accel, err);
+    return cudaGetLastError();
+}
+
+uint32_t conservation_blocks(uint32_t n) {
+    uint32_t blocks = (n + kConsThreads - 1) / kConsThreads;
+    return blocks < 592u ? (blocks ? blocks : 1u) : 592u;
+}
+
+cudaError_t launch_conservation(const GpuEvolveState* state, const float* potential, uint32_t n,
+                                double* partials, uint32_t nblocks, double* out,
+                                cudaStream_t s) {
+    k_conservation_partial<<<nblocks, kConsThreads, 0, s>>>(state, potential, n, partials);
+    k_conservation_final<<<1, 32, 0, s>>>(partials, nblocks, out);
+    return cudaGetLastError();
+}
+
+}  // namespace gbh

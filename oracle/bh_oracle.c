@@ -10,6 +10,7 @@
  * Compile with -O2 -ffp-contract=off: each f64 expression below is written in
  * the reference's evaluation order and must round exactly as Rust does.
  */
+#define _POSIX_C_SOURCE 200809L
 #include "bh_oracle.h"
 
 #include <math.h>
@@ -18,6 +19,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 static __thread char g_err[512];
 
@@ -335,6 +337,29 @@ uint64_t ob_flat_topology_checksum(const ob_flat_tree* t) {
         checksum_word(&hash, cell->end);
         checksum_word(&hash, cell->depth);
         for (int q = 0; q < 4; ++q) checksum_word(&hash, cell->children[q]);
+    }
+    return hash;
+}
+
+/* flat.rs:416-433 over arrays: entries as (code, body_index) pairs and cells
+ * as frozen 16-word GpuCell records (range_depth at words 8..10, children at
+ * 12..15), so a GPU-built tree can be checksummed the reference's way. */
+uint64_t ob_topology_checksum_arrays(uint32_t n, const uint32_t* entries_pairs,
+                                     uint32_t entry_stride, uint32_t ncells,
+                                     const uint32_t* cells16) {
+    uint64_t hash = 0xcbf29ce484222325ull;
+    checksum_word(&hash, OB_MORTON_AXIS_BITS);
+    checksum_word(&hash, n);
+    for (uint32_t i = 0; i < n; ++i) {
+        checksum_word(&hash, entries_pairs[(size_t)i * entry_stride + 0]);
+        checksum_word(&hash, entries_pairs[(size_t)i * entry_stride + 1]);
+    }
+    for (uint32_t k = 0; k < ncells; ++k) {
+        const uint32_t* c = cells16 + 16 * (size_t)k;
+        checksum_word(&hash, c[8]);
+        checksum_word(&hash, c[9]);
+        checksum_word(&hash, c[10]);
+        for (int q = 0; q < 4; ++q) checksum_word(&hash, c[12 + q]);
     }
     return hash;
 }
@@ -890,6 +915,41 @@ int ob_cpu_flat_evolve(ob_body* b, size_t n, size_t steps, double dt, const ob_c
     }
     free(acc);
     return rc;
+}
+
+/* The loop body of galaxy-bh-evolve.rs:348-361: `steps` KDK steps from a
+ * boundary acceleration `acc` (n rows, updated in place), so steps can be
+ * timed one at a time.  build_seconds/force_seconds (optional) accumulate the
+ * tree-build and traversal wall times. */
+int ob_cpu_flat_steps(ob_body* b, size_t n, ob_accel* acc, size_t steps, double dt,
+                      const ob_config* c, int nthreads, double* build_seconds,
+                      double* force_seconds) {
+    struct timespec t0, t1, t2;
+    for (size_t s = 0; s < steps; ++s) {
+        for (size_t i = 0; i < n; ++i) {
+            b[i].vx += 0.5 * dt * acc[i].ax;
+            b[i].vy += 0.5 * dt * acc[i].ay;
+            b[i].x += dt * b[i].vx;
+            b[i].y += dt * b[i].vy;
+        }
+        ob_flat_tree* t = NULL;
+        clock_gettime(CLOCK_MONOTONIC, &t0);
+        int rc = ob_flat_tree_build(b, n, c, &t);
+        clock_gettime(CLOCK_MONOTONIC, &t1);
+        if (!rc) rc = ob_flat_accelerations(b, n, t, c, NULL, 0, acc, NULL, NULL, nthreads);
+        clock_gettime(CLOCK_MONOTONIC, &t2);
+        ob_flat_tree_free(t);
+        if (rc) return rc;
+        if (build_seconds)
+            *build_seconds += (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
+        if (force_seconds)
+            *force_seconds += (double)(t2.tv_sec - t1.tv_sec) + 1e-9 * (double)(t2.tv_nsec - t1.tv_nsec);
+        for (size_t i = 0; i < n; ++i) {
+            b[i].vx += 0.5 * dt * acc[i].ax;
+            b[i].vy += 0.5 * dt * acc[i].ay;
+        }
+    }
+    return 0;
 }
 
 /* galaxy-bh-evolve.rs:252-278 */

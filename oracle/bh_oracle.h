@@ -85,6 +85,11 @@ void ob_flat_tree_copy(const ob_flat_tree* t, ob_entry* entries, uint32_t* posit
                        ob_cell* cells);
 /* nbody/src/flat.rs:416-433 */
 uint64_t ob_flat_topology_checksum(const ob_flat_tree* t);
+/* The same checksum over (code, body_index) words (entry_stride words per
+ * entry) and 16-word GpuCell records. */
+uint64_t ob_topology_checksum_arrays(uint32_t n, const uint32_t* entries_pairs,
+                                     uint32_t entry_stride, uint32_t ncells,
+                                     const uint32_t* cells16);
 
 /* nbody/src/flat.rs:270-371.  targets==NULL: all bodies (out has n rows),
  * else out has ntargets rows.  abs_sum (optional) receives, per target, the
@@ -128,6 +133,12 @@ int ob_pack_flat_tree(const ob_body* b, size_t n, const ob_flat_tree* t, const o
 /* runtime/src/bin/galaxy-bh-evolve.rs:339-363 (f64 KDK on the flat tree). */
 int ob_cpu_flat_evolve(ob_body* b, size_t n, size_t steps, double dt, const ob_config* c,
                        int nthreads);
+
+/* `steps` KDK steps from the boundary acceleration acc (updated in place):
+ * the loop body of galaxy-bh-evolve.rs:348-361. */
+int ob_cpu_flat_steps(ob_body* b, size_t n, ob_accel* acc, size_t steps, double dt,
+                      const ob_config* c, int nthreads, double* build_seconds,
+                      double* force_seconds);
 
 /* runtime/src/bin/galaxy-bh-evolve.rs:252-278: mass, com_x, com_y, px, py, lz,
  * mass_speed_scale. */

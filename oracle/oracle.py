@@ -115,6 +115,8 @@ def lib():
         L.ob_flat_tree_copy.restype = None
         L.ob_flat_topology_checksum.argtypes = [P]
         L.ob_flat_topology_checksum.restype = C.c_uint64
+        L.ob_topology_checksum_arrays.argtypes = [C.c_uint32, P, C.c_uint32, C.c_uint32, P]
+        L.ob_topology_checksum_arrays.restype = C.c_uint64
         L.ob_flat_accelerations.argtypes = [P, sz, P, cfg, P, sz, P, P, C.POINTER(_ForceStats),
                                             C.c_int]
         L.ob_direct_acceleration_for.argtypes = [sz, P, sz, cfg, P]
@@ -130,6 +132,8 @@ def lib():
         L.ob_state_checksum.restype = C.c_uint64
         L.ob_pack_flat_tree.argtypes = [P, sz, P, cfg, P, P, P, P]
         L.ob_cpu_flat_evolve.argtypes = [P, sz, sz, C.c_double, cfg, C.c_int]
+        L.ob_cpu_flat_steps.argtypes = [P, sz, P, sz, C.c_double, cfg, C.c_int,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ob_invariants.argtypes = [P, sz, P]
         L.ob_invariants.restype = None
         L.ob_f32_kick_drift.argtypes = [P, P, sz, C.c_float]
@@ -240,6 +244,15 @@ def build_flat_tree(bodies, cfg: Config) -> FlatTree:
     return FlatTree(entries, pos, cells, info.root, info.stats.node_count, info.stats.leaf_count,
                     info.stats.max_depth, (info.root_cx, info.root_cy, info.root_half),
                     int(lib().ob_flat_topology_checksum(h)), handle)
+
+
+def topology_checksum_arrays(entry_words: np.ndarray, cells16: np.ndarray) -> int:
+    """flat_topology_checksum (flat.rs:416-433) of a tree given as raw words:
+    entry_words (n, k>=2) u32 with code, body_index first; cells16 (C, 16) u32
+    GpuCell records."""
+    e = np.ascontiguousarray(entry_words, dtype=np.uint32)
+    c = np.ascontiguousarray(cells16, dtype=np.uint32).reshape(-1, 16)
+    return int(lib().ob_topology_checksum_arrays(len(e), _ptr(e), e.shape[1], len(c), _ptr(c)))
 
 
 def flat_accelerations(bodies, tree: FlatTree, cfg: Config, targets=None, abs_sum=False,
@@ -401,6 +414,18 @@ def cpu_flat_evolve(bodies, steps: int, dt: float, cfg: Config, nthreads=1) -> n
     b = _bodies(bodies).copy()
     _check(lib().ob_cpu_flat_evolve(_ptr(b), len(b), steps, dt, C.byref(cfg), nthreads))
     return b
+
+
+def cpu_flat_steps(bodies: np.ndarray, acc: np.ndarray, steps: int, dt: float, cfg: Config,
+                   nthreads=1) -> tuple[float, float]:
+    """In place: ``steps`` KDK steps of bodies (n,5) from boundary acc (n,2)
+    (galaxy-bh-evolve.rs:348-361).  Returns (build_seconds, force_seconds)."""
+    assert bodies.dtype == np.float64 and bodies.flags.c_contiguous
+    assert acc.dtype == np.float64 and acc.flags.c_contiguous and acc.shape == (len(bodies), 2)
+    tb, tf = C.c_double(0.0), C.c_double(0.0)
+    _check(lib().ob_cpu_flat_steps(_ptr(bodies), len(bodies), _ptr(acc), steps, dt,
+                                   C.byref(cfg), nthreads, C.byref(tb), C.byref(tf)))
+    return tb.value, tf.value
 
 
 def f32_kick_drift(states: np.ndarray, accel: np.ndarray, dt: float) -> np.ndarray:

@@ -1,0 +1,315 @@
+"""CUDA engine vs the CPU oracle, through the C ABI (via the host mirror).
+
+Bit-exact: Morton codes, sort permutation, Morton positions, the whole
+frozen cell layout (including the f64->f32 aggregates and centres), the
+topology checksum, the f32 kick/drift stages.  Toleranced: per-body forces
+(f32 arithmetic vs the f64 reference traversal on the same tree and theta).
+Force tolerance, per body i:  |a_gpu - a_ref| <= 1e-5 * |a_ref| + 2e-6 * S_i,
+S_i = sum of the magnitudes of body i's terms (each f32 term carries a few
+ulp of its own magnitude, so a body whose terms cancel to a small net force
+cannot do better in f32); over all bodies the plain relative error
+|a_gpu - a_ref| / |a_ref| must have median <= 1e-6 and 99th percentile
+<= 1e-5.
+"""
+import numpy as np
+import pytest
+
+from galaxy_b200 import scenarios
+from galaxy_b200.nbody_gpu import (Config, NbodyGpu, ParallelTreeRuntime, bodies_to_state,
+                                   pack_flat_tree, state_to_bodies)
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL = 1e-5
+FORCE_ABS_SUM = 2e-6
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    g = NbodyGpu()
+    yield g
+
+
+@pytest.fixture(scope="module")
+def rt(gpu):
+    return ParallelTreeRuntime(gpu)
+
+
+def f32_bodies(bodies):
+    """The f32 state the engine holds, promoted back to f64."""
+    return state_to_bodies(bodies_to_state(bodies))
+
+
+def ocfg(oracle, cfg: Config):
+    return oracle.Config(theta=cfg.theta, softening=cfg.softening_kpc, g=cfg.g,
+                         bucket=cfg.bucket, max_depth=cfg.max_depth)
+
+
+def build_both(gpu, rt, oracle, bodies, cfg):
+    b32 = f32_bodies(bodies)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    evid = rt.read_evidence(gpu, tree)
+    oc = ocfg(oracle, cfg)
+    ot = oracle.build_flat_tree(b32, oc)
+    return ev, tree, evid, ot, b32, oc
+
+
+def assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg):
+    packed = oracle.pack_flat_tree(b32, ot, oc)
+    e = evid.entries["data"]
+    assert np.array_equal(e[:, 0], ot.codes), "Morton codes differ"
+    assert np.array_equal(e[:, 1], ot.order), "sort permutation differs"
+    assert np.array_equal(evid.bodies["meta"][:, 0], ot.position_by_body)
+    assert np.array_equal(evid.bodies.view(np.uint32).reshape(-1, 8), packed.bodies)
+    assert evid.active_cell_count == len(ot.cells)
+    gc = evid.cells.view(np.uint32).reshape(-1, 16)
+    assert np.array_equal(gc[:, 8:16], packed.cells[:, 8:16]), "topology differs"
+    assert np.array_equal(gc, packed.cells), "cell aggregates/centres differ"
+    gpu_sum = oracle.topology_checksum_arrays(e, gc)
+    assert gpu_sum == ot.checksum
+    assert evid.max_depth == ot.max_depth
+    assert evid.leaf_count == ot.leaf_count
+
+
+def force_check(oracle, acc_gpu, b32, ot, oc, targets=None):
+    ref, stats, s = oracle.flat_accelerations(b32, ot, oc, targets=targets, abs_sum=True)
+    a = acc_gpu if targets is None else acc_gpu[targets]
+    err = np.hypot(a[:, 0] - ref[:, 0], a[:, 1] - ref[:, 1])
+    mag = np.hypot(ref[:, 0], ref[:, 1])
+    bound = FORCE_REL * mag + FORCE_ABS_SUM * s
+    assert (err <= bound).all(), f"worst err/bound {np.max(err / np.maximum(bound, 1e-300))}"
+    rel = err / np.maximum(mag, 1e-30)
+    assert np.quantile(rel, 0.99) <= FORCE_REL, f"p99 rel {np.quantile(rel, 0.99)}"
+    assert np.median(rel) <= 1e-6, f"median rel {np.median(rel)}"
+    return rel, stats
+
+
+def _ref_disc(oracle, n, seed):
+    return oracle.make_disc(n, seed, 5.0e10, 3.0)
+
+
+@pytest.mark.parametrize("n,bucket,max_depth", [
+    (2, 1, 48), (3, 1, 48), (100, 1, 48), (1000, 4, 48), (4099, 16, 48), (5000, 1, 5),
+    (3000, 2, 1), (20000, 1, 48), (70000, 8, 12),
+])
+def test_tree_bit_exact_reference_disc(gpu, rt, oracle, n, bucket, max_depth):
+    cfg = Config(bucket=bucket, max_depth=max_depth)
+    bodies = _ref_disc(oracle, max(n, 2), 303 + n)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+
+
+@pytest.mark.parametrize("scenario,n", [("exponential_disc", 16384), ("cold_disc", 30000),
+                                        ("binary_encounter", 20000)])
+def test_tree_bit_exact_scenarios(gpu, rt, oracle, scenario, n):
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1, max_depth=48)
+    bodies = scenarios.make(scenario, n, 42)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+
+
+def test_coincident_bodies_keep_order_and_reach_depth_16(gpu, rt, oracle):
+    # flat.rs:483-506 on the GPU builder
+    bodies = np.array([[0.0, 0.0, 0.0, 0.0, 1.0]] * 8 + [[1.0, 1.0, 0.0, 0.0, 1.0]])
+    cfg = Config(bucket=1, max_depth=48, softening_kpc=0.1)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+    assert list(evid.entries["data"][:8, 1]) == list(range(8))
+    assert evid.max_depth == 16
+
+
+def test_clustered_pairs_hit_depth_limit(gpu, rt, oracle):
+    rng = np.random.default_rng(5)
+    centers = rng.uniform(-1, 1, (3000, 2))
+    pts = np.concatenate([centers, centers + 1e-6], axis=0)
+    bodies = np.zeros((len(pts), 5))
+    bodies[:, :2] = pts
+    bodies[:, 4] = 1.0 / len(pts)
+    for bucket in (1, 3):
+        cfg = Config(bucket=bucket, g=1.0, softening_kpc=0.01)
+        ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+        assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.3, 0.5, 0.7, 2.0])
+def test_forces_match_reference_traversal(gpu, rt, oracle, theta):
+    cfg = Config(theta=theta, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.exponential_disc(8192 if theta > 0 else 2048, 42)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    rel, stats = force_check(oracle, acc, b32, ot, oc)
+    gs = rt.force_stats(gpu, tree)
+    # identical opening decisions: the same cells visited, approximated, summed
+    assert gs["visited_nodes"] == stats["visited_nodes"]
+    assert gs["approximated_cells"] == stats["approximated_cells"]
+    assert gs["direct_terms"] == stats["direct_terms"]
+
+
+@pytest.mark.parametrize("bucket", [4, 16])
+def test_forces_reference_units_and_buckets(gpu, rt, oracle, bucket):
+    cfg = Config(bucket=bucket)  # kpc units, eps 0.05, G of lib.rs:6
+    bodies = oracle.make_collision(6000, 77)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    rel, stats = force_check(oracle, acc, b32, ot, oc)
+    gs = rt.force_stats(gpu, tree)
+    assert gs["approximated_cells"] == stats["approximated_cells"]
+    assert gs["direct_terms"] == stats["direct_terms"]
+
+
+def test_compensated_forces_tighter(gpu, rt, oracle):
+    cfg = Config(theta=0.5, softening_kpc=0.005, g=1.0, bucket=1, compensated=True)
+    bodies = scenarios.cold_disc(16384, 7)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    rel, _ = force_check(oracle, acc, b32, ot, oc)
+    assert np.median(rel) < 1e-6
+
+
+def test_kick_drift_final_kick_bit_exact(gpu, oracle):
+    bodies = scenarios.exponential_disc(5000, 3)
+    s0 = bodies_to_state(bodies)
+    ev, _ = gpu.create_evolving_state(bodies)
+    rng = np.random.default_rng(1)
+    acc = np.zeros((5000, 4), np.float32)
+    acc[:, :2] = rng.normal(0, 3, (5000, 2)).astype(np.float32)
+    # load an arbitrary acceleration through the packed-force path is not
+    # needed: write state, then integrate against the engine's own accel
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    rt = ParallelTreeRuntime(gpu)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    a32, _ = gpu.read_evolving_accelerations_f32(ev)
+    recs = s0.view(np.float32).reshape(-1, 8)
+    gpu.kick_drift(ev, 1e-3)
+    got, _ = gpu.read_evolving_state_records(ev)
+    want = oracle.f32_kick_drift(recs, a32, 1e-3)
+    assert np.array_equal(got.view(np.float32).reshape(-1, 8), want)
+    gpu.final_kick(ev, 1e-3)
+    got2, _ = gpu.read_evolving_state_records(ev)
+    want2 = oracle.f32_final_kick(want, a32, 1e-3)
+    assert np.array_equal(got2.view(np.float32).reshape(-1, 8), want2)
+    if oracle.ref_cuda() is not None:
+        # barnes_hut_flat.cu:149-185 built with nvcc's default FMA contraction:
+        # v + (0.5*dt)*a and x + dt*v fuse, so it may differ by one rounding.
+        # A fused rounding differs by at most one ulp of the product 0.5*dt*a
+        # (~5e-10 here), which cancellation can make large relative to v.
+        r = oracle.ref_cuda_integrate(recs, a32, 1e-3)
+        np.testing.assert_allclose(r, want, rtol=5e-7, atol=2e-9)
+
+
+def test_packed_path_matches_models(gpu, oracle):
+    bodies = oracle.make_disc(3000, 303, 5.0e10, 3.0)
+    oc = oracle.Config()
+    b32 = f32_bodies(bodies)
+    ot = oracle.build_flat_tree(b32, oc)
+    cfg = Config()
+    packed = pack_flat_tree(b32, ot, cfg)
+    op = oracle.pack_flat_tree(b32, ot, oc)
+    assert packed.bodies.view(np.uint32).reshape(-1, 8).tobytes() == op.bodies.tobytes()
+    assert packed.cells.view(np.uint32).reshape(-1, 16).tobytes() == op.cells.tobytes()
+    res = gpu.traverse(packed)
+    model = oracle.f32_traverse_packed(op)[:, :2].astype(np.float64)
+    ref64, _ = oracle.flat_accelerations(b32, ot, oc)
+    rel_model = oracle.relative_errors(res.accelerations, model)
+    assert np.quantile(rel_model, 0.99) < 1e-5
+    rel64 = oracle.relative_errors(res.accelerations, ref64)
+    assert np.sqrt(np.mean(rel64 ** 2)) < 0.01 and rel64.max() < 0.10  # galaxy-bh-gpu.rs:109
+    if oracle.ref_cuda() is not None:
+        ref_gpu, _ = oracle.ref_cuda_traverse(op)
+        rel_ref = oracle.relative_errors(res.accelerations, ref_gpu[:, :2].astype(np.float64))
+        assert np.quantile(rel_ref, 0.999) < 1e-5
+
+
+def test_repeat_rebuild_bit_identical(gpu, rt, oracle):
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.binary_encounter(40000, 9)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    a = rt.read_evidence(gpu, tree)
+    rt.force(gpu, ev, tree, cfg)
+    f1, _ = gpu.read_evolving_accelerations(ev)
+    rt.rebuild(gpu, ev, tree, cfg)
+    b = rt.read_evidence(gpu, tree)
+    rt.force(gpu, ev, tree, cfg)
+    f2, _ = gpu.read_evolving_accelerations(ev)
+    assert a.cells.tobytes() == b.cells.tobytes() and a.entries.tobytes() == b.entries.tobytes()
+    assert np.array_equal(f1, f2)
+
+
+def _unfused_steps(gpu, rt, ev, tree, cfg, dt, steps):
+    for _ in range(steps):
+        gpu.kick_drift(ev, dt)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        gpu.final_kick(ev, dt)
+
+
+def test_fused_step_equals_reference_loop(gpu, rt):
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.exponential_disc(12000, 42)
+    evs = []
+    for fused in (False, True):
+        ev, _ = gpu.create_evolving_state(bodies)
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        if fused:
+            rt.step(gpu, ev, tree, cfg, 1e-3, 5)
+        else:
+            _unfused_steps(gpu, rt, ev, tree, cfg, 1e-3, 5)
+        evs.append((gpu.read_evolving_state_records(ev)[0],
+                    gpu.read_evolving_accelerations_f32(ev)[0]))
+    assert evs[0][0].tobytes() == evs[1][0].tobytes()
+    assert np.array_equal(evs[0][1], evs[1][1])
+
+
+def test_evolution_trajectory_gates(gpu, rt, oracle):
+    # galaxy-bh-gpu-tree-parallel.rs:372-415 gates on the reference disc
+    bodies = oracle.make_disc(2048, 303, 5.0e10, 3.0)
+    cfg = Config(theta=0.5)
+    oc = ocfg(oracle, cfg)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    rt.step(gpu, ev, tree, cfg, 0.01, 3)
+    final, _ = gpu.read_evolving_state(ev)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    rms, mx = oracle.probe_error(final, acc, oc, 12)
+    assert rms < 0.04 and mx < 0.30
+    ref = oracle.cpu_flat_evolve(bodies, 3, 0.01, oc)
+    pd = np.hypot(final[:, 0] - ref[:, 0], final[:, 1] - ref[:, 1])
+    pr = np.hypot(ref[:, 0], ref[:, 1])
+    vd = np.hypot(final[:, 2] - ref[:, 2], final[:, 3] - ref[:, 3])
+    vr = np.hypot(ref[:, 2], ref[:, 3])
+    assert np.sqrt((pd ** 2).sum() / (pr ** 2).sum()) < 0.03
+    assert (pd / np.maximum(pr, 1e-6)).max() < 0.30
+    assert np.sqrt((vd ** 2).sum() / (vr ** 2).sum()) < 0.03
+    assert (vd / np.maximum(vr, 1e-9)).max() < 0.30
+    # and the tree of the final f32 state is the reference's, bit for bit
+    rt.rebuild(gpu, ev, tree, cfg)
+    evid = rt.read_evidence(gpu, tree)
+    ot = oracle.build_flat_tree(final, oc)
+    assert_tree_bit_exact(oracle, evid, ot, final, oc, cfg)
+
+
+def test_conservation_f64(gpu):
+    bodies = scenarios.exponential_disc(10000, 2)
+    ev, _ = gpu.create_evolving_state(bodies)
+    c = gpu.conservation(ev)
+    b = f32_bodies(bodies)
+    m = b[:, 4]
+    assert c["mass"] == pytest.approx(m.sum(), rel=1e-13)
+    assert c["px"] == pytest.approx((m * b[:, 2]).sum(), rel=1e-10, abs=1e-14)
+    lz = (m * (b[:, 0] * b[:, 3] - b[:, 1] * b[:, 2])).sum()
+    assert c["lz"] == pytest.approx(lz, rel=1e-12)
+    ke = 0.5 * (m * (b[:, 2] ** 2 + b[:, 3] ** 2)).sum()
+    assert c["kinetic"] == pytest.approx(ke, rel=1e-12)
