@@ -49,6 +49,10 @@ static int cuda_fail(cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(_e, what); \
     } while (0)
 
+int gbh::set_error_message(int status, const char* message) {
+    return set_error(status, "%s", message);
+}
+
 extern "C" size_t galaxy_bh_last_error(char* buf, size_t len) {
     if (buf && len) {
         size_t n = std::min(len - 1, g_last_error.size());

@@ -121,4 +121,7 @@ cudaError_t launch_conservation(const GpuEvolveState* state, const float* potent
                                 cudaStream_t s);
 uint32_t conservation_blocks(uint32_t n);
 
+// Sets the calling thread's last-error message (bh_engine.cu); returns status.
+int set_error_message(int status, const char* message);
+
 }  // namespace gbh

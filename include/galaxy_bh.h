@@ -216,6 +216,23 @@ int galaxy_bh_step(bh_device* dev, bh_state* st, bh_tree* tree, const bh_config*
  * first six follow galaxy-bh-evolve.rs:252-278. */
 int galaxy_bh_conservation(bh_device* dev, bh_state* st, double out[10]);
 
+/* The same sums for callers that cannot allocate device memory — a serving
+ * loop that reserved its memory budget up front, a host whose own allocator
+ * owns the device memory, code handed only device buffers.  No counterpart in
+ * the reference (it has no allocation-free path).  Allocates nothing: state
+ * (n GpuEvolveState records) and potential (n floats, or NULL) are device
+ * inputs; sums is a device output of 9 doubles — mass, sum m*x, sum m*y, px,
+ * py, lz, kinetic, potential, sum m*|v| (divide 1 and 2 by 0 for the centre
+ * of mass).  Work is enqueued on `stream` (a cudaStream_t; NULL = default
+ * stream) and the function returns without waiting.  Scratch is a 73,728-byte
+ * static device array, so n is limited to 4,194,304 (BH_INVALID_ARG beyond).
+ * The first call on each device looks up that array's device address with
+ * the device current; make that first call before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (different streams
+ * or threads at once) race and corrupt each other's sums. */
+int galaxy_bh_conservation_noalloc(const GpuEvolveState* state, const float* potential,
+                                   uint32_t n, double* sums, void* stream);
+
 /* ---- batched engine --------------------------------------------------------
  * Many independent simulations of uneven n advanced together: one launch per
  * stage covers every simulation.  Each state keeps its own resident buffers;
