@@ -345,7 +345,11 @@ def run_engine(args, world, rank, local, pg):
                       "peak_tflops": fp32_peak, "peak_source": "nominal FP32 at sampled clock",
                       "frac": flops / stage["traverse"] / 1e12 / fp32_peak,
                       "share_of_step": stage["traverse"] / (ms * 1e-3 / args.steps),
-                      "cells_per_body": c, "exact_mac_fallbacks": fstats["exact_mac_fallbacks"]},
+                      "cells_per_body": c, "exact_mac_fallbacks": fstats["exact_mac_fallbacks"],
+                      "lane_visits": fstats["visited_nodes"],
+                      "warp_iterations": fstats["warp_iterations"],
+                      "union_over_lane": 32.0 * fstats["warp_iterations"] /
+                      max(1, fstats["visited_nodes"])},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 32 * N_BODIES,
                 "d2h_bytes_per_step": 32 * N_BODIES, "steps": e2e_steps,
                 "how": "per step: galaxy_bh_write_state from pinned host, one fused KDK step, "

@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgalaxy_bh.so")
+# GALAXY_BH_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("GALAXY_BH_LIB") or os.path.join(HERE, "libgalaxy_bh.so")
 
 NO_CHILD = 0xFFFFFFFF
 
@@ -78,7 +79,8 @@ class BhBuildTiming(C.Structure):
 
 class BhForceStats(C.Structure):
     _fields_ = [("visited_nodes", C.c_uint64), ("approximated_cells", C.c_uint64),
-                ("direct_terms", C.c_uint64), ("exact_mac_fallbacks", C.c_uint64)]
+                ("direct_terms", C.c_uint64), ("exact_mac_fallbacks", C.c_uint64),
+                ("warp_iterations", C.c_uint64)]
 
 
 # name -> (restype, argtypes); every exported symbol of include/galaxy_bh.h.

@@ -490,6 +490,9 @@ struct Batch {
     cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
     uint32_t graph_flags = 0xffffffffu;
     bool stats_valid = false;
+    // theta and G the cell records (G*m, MAC bounds) were last computed with
+    // (single-simulation trees; batches keep their creation configs)
+    double built_theta = NAN, built_g = NAN;
 
     ~Batch() {
         for (auto& g : graphs)
@@ -524,11 +527,11 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Byte sizes of the arena regions, in carve order.
 struct ArenaPlan {
-    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_f, cell_u, cell_d,
-        cell_child, cell_parent, cell_counter, err, stats;
+    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_r, cell_end,
+        cell_d, cell_child, cell_parent, cell_counter, err, stats;
     size_t total() const {
         return control + sims + simout + chunk + tiles + 2 * keys + 2 * vals + sbody + base +
-               cell_f + cell_u + cell_d + cell_child + cell_parent + cell_counter + err + stats;
+               cell_r + cell_end + cell_d + cell_child + cell_parent + cell_counter + err + stats;
     }
 };
 
@@ -545,8 +548,8 @@ static ArenaPlan plan_arena(const Layout& L, uint32_t nsims) {
     a.vals = align256(4ull * L.npos);
     a.sbody = align256(16ull * L.npos);
     a.base = align256(4ull * (L.npos + 1));
-    a.cell_f = align256(16ull * L.cells);
-    a.cell_u = align256(16ull * L.cells);
+    a.cell_r = align256(sizeof(CellRec) * L.cells);
+    a.cell_end = align256(4ull * L.cells);
     a.cell_d = align256(32ull * L.cells);
     a.cell_child = align256(16ull * L.cells);
     a.cell_parent = align256(4ull * L.cells);
@@ -630,8 +633,8 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.vals_b = (uint32_t*)take(A.vals);
     bb.sbody = (float4*)take(A.sbody);
     bb.base = (uint32_t*)take(A.base);
-    bb.cell_f = (float4*)take(A.cell_f);
-    bb.cell_u = (uint4*)take(A.cell_u);
+    bb.cell_r = (CellRec*)take(A.cell_r);
+    bb.cell_end = (uint32_t*)take(A.cell_end);
     bb.cell_d = (double4*)take(A.cell_d);
     bb.cell_child = (uint4*)take(A.cell_child);
     bb.cell_parent = (uint32_t*)take(A.cell_parent);
@@ -740,7 +743,7 @@ static bool any_flag(Batch* b, uint32_t flag) {
 
 static int enqueue_force(Batch* b, bool stats) {
     cudaStream_t s = b->dev->stream;
-    if (stats) CK(cudaMemsetAsync(b->bb.force_stats, 0, 32, s), "memset");
+    if (stats) CK(cudaMemsetAsync(b->bb.force_stats, 0, 40, s), "memset");
     CK(launch_traverse(b->bb, any_flag(b, BH_FLAG_COMPENSATED), any_flag(b, BH_FLAG_POTENTIAL),
                        stats, s),
        "traverse launch");
@@ -884,6 +887,8 @@ extern "C" int galaxy_bh_tree_rebuild(bh_device* dev, bh_state* st, bh_tree* tre
         timing->aggregate_seconds = ms[4] * 1e-3;
     }
     tree->built = true;
+    tree->batch->built_theta = cfg->theta;
+    tree->batch->built_g = cfg->g;
     return BH_OK;
 }
 
@@ -893,6 +898,12 @@ extern "C" int galaxy_bh_force(bh_device* dev, bh_state* st, bh_tree* tree, cons
     if (rc) return rc;
     if (!tree->built) return set_error(BH_INVALID_ARG, "force requires a rebuilt tree");
     if ((rc = apply_configs(tree->batch, cfg, false))) return rc;
+    Batch* b = tree->batch;
+    if (cfg->theta != b->built_theta || cfg->g != b->built_g) {
+        CK(launch_refresh_mac(b->bb, 0, dev->stream), "refresh launch");
+        b->built_theta = cfg->theta;
+        b->built_g = cfg->g;
+    }
     CK(cudaEventRecord(dev->ev[0], dev->stream), "event");
     if ((rc = enqueue_force(tree->batch, true))) return rc;
     if ((rc = stage_time(dev, timing))) return rc;
@@ -906,7 +917,7 @@ extern "C" int galaxy_bh_force_stats(bh_device* dev, bh_tree* tree, bh_force_sta
     if (!tree || !out) return set_error(BH_INVALID_ARG, "null argument");
     if (!tree->batch->stats_valid)
         return set_error(BH_INVALID_ARG, "no force statistics since the last galaxy_bh_force");
-    unsigned long long v[4];
+    unsigned long long v[5];
     CK(cudaMemcpyAsync(v, tree->batch->bb.force_stats, sizeof v, cudaMemcpyDeviceToHost,
                        dev->stream),
        "readback");
@@ -915,6 +926,7 @@ extern "C" int galaxy_bh_force_stats(bh_device* dev, bh_tree* tree, bh_force_sta
     out->approximated_cells = v[1];
     out->direct_terms = v[2];
     out->exact_mac_fallbacks = v[3];
+    out->warp_iterations = v[4];
     return BH_OK;
 }
 
@@ -987,6 +999,8 @@ extern "C" int galaxy_bh_step(bh_device* dev, bh_state* st, bh_tree* tree, const
     if (nsteps == 0) return BH_OK;
     tree->batch->h_sims[0].dt = f;
     if ((rc = apply_configs(tree->batch, cfg, true))) return rc;
+    tree->batch->built_theta = cfg->theta;
+    tree->batch->built_g = cfg->g;
     return run_graphs(tree->batch, nsteps);
 }
 

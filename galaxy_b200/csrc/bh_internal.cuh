@@ -56,6 +56,17 @@ struct SimOut {
     double reserved;
 };
 
+// Traversal record of one cell (32 bytes, one sector):
+//   f = (com_x, com_y, G*mass, hi) in f32, with the cell depth in the low 5
+//       bits of hi (hi rounded up to make room, so the MAC band only widens)
+//   u = (lo as f32 bits | leaf body count, skip, start, depth)
+// hi is -1 for a one-body leaf and +inf (a NaN once depth is packed) for a
+// leaf of several bodies; skip = index of the next cell after the subtree.
+struct CellRec {
+    float4 f;
+    uint4 u;
+};
+
 struct Tile {
     uint32_t sim;
     uint32_t start;  // first position
@@ -88,8 +99,8 @@ struct BatchBuffers {
     uint32_t* vals_b;
     float4* sbody;      // sorted (x, y, m, body index bits)
     uint32_t* base;     // npos + 1: first cell index of each position's chain
-    float4* cell_f;     // com_x, com_y, mass, width (f32)
-    uint4* cell_u;      // start, end, skip, depth (global positions)
+    CellRec* cell_r;    // traversal records
+    uint32_t* cell_end; // end position (build and export only)
     double4* cell_d;    // com_x, com_y, mass, 0 (f64)
     uint4* cell_child;  // children (global cell indices)
     uint32_t* cell_parent;
@@ -107,6 +118,8 @@ cudaError_t launch_radix(const BatchBuffers& b, cudaStream_t s);
 cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s);
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s);
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s);
+// Recomputes G*m and the MAC bounds of simulation `sim` for new theta / G.
+cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s);
 cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
                             cudaStream_t s);
 cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,

@@ -569,9 +569,10 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
                                                const uint32_t* __restrict__ chunk_sim,
                                                uint32_t npos, uint32_t capacity,
                                                const uint32_t* __restrict__ codes,
-                                               const uint32_t* __restrict__ base, uint4* cell_u,
-                                               uint4* cell_child, uint32_t* cell_parent,
-                                               uint32_t* cell_counter, uint32_t* err) {
+                                               const uint32_t* __restrict__ base, CellRec* cell_r,
+                                               uint32_t* cell_end, uint4* cell_child,
+                                               uint32_t* cell_parent, uint32_t* cell_counter,
+                                               uint32_t* err) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npos) return;
     const uint32_t s = chunk_sim[p >> 5];
@@ -600,7 +601,9 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
     for (uint32_t d = dmin; d <= deepest; ++d) {
         const uint32_t k = k0 + (d - dmin);
         const uint32_t end = ends[d - dmin];
-        cell_u[k] = make_uint4(p, sd.off + end, base[sd.off + end], d);
+        // u.x (MAC lower bound or leaf body count) and f are filled by k_aggregate
+        cell_r[k].u = make_uint4(0u, base[sd.off + end], p, d);
+        cell_end[k] = sd.off + end;
         cell_counter[k] = 0;
         uint4 ch = make_uint4(kNone, kNone, kNone, kNone);
         if (d < deepest) {
@@ -635,14 +638,76 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
 
 // =========================================================== aggregate ====
 
+// Guard band of the f32 opening test.  The exact test (flat.rs:317-323) opens
+// a cell unless width/dist < theta, i.e. approximates iff dist^2 > crit^2 with
+// crit = width/theta.  The traversal computes d2 in f32 from the f32 centre of
+// mass; with u = 2^-24 and C = |com_x| + |com_y| its error is at most
+// 2u*C*d + 4u*d^2, and d <= (d^2 + crit^2)/(2 crit) turns that into a bound
+// linear in d^2: |d2_f32 - d^2| <= d^2 * r + u*C*crit, r = u*C/crit + 4u.
+// So d2_f32 > hi proves "approximate" and d2_f32 < lo proves "open" (with a
+// 4x margin and 1e-4 relative slack); in between the traversal decides in f64.
+__device__ __forceinline__ void mac_band(double width, double theta, float com_x, float com_y,
+                                         float* lo, float* hi) {
+    if (!(theta > 0.0)) {  // theta = 0: every cell opens
+        *lo = INFINITY;
+        *hi = INFINITY;
+        return;
+    }
+    const double crit = width / theta;
+    const double crit2 = crit * crit;
+    if (!(crit2 < 1e38)) {  // beyond any f32 distance: always open
+        *lo = INFINITY;
+        *hi = INFINITY;
+        return;
+    }
+    const double u = 5.9604644775390625e-8;
+    const double C = fabs((double)com_x) + fabs((double)com_y);
+    const double r = u * C / crit + 4.0 * u;
+    const double slack = 4.0 * r + 1e-4;
+    *hi = __double2float_ru(crit2 * (1.0 + slack) + 4.0 * u * C * crit);
+    *lo = __double2float_rd(crit2 * (1.0 - slack) - 4.0 * u * C * crit);
+}
+
+// hi with the depth in its low 5 bits, rounded away from zero to make room:
+// a larger positive bound (or a more negative -1) only widens the band, and
+// +inf becomes a NaN, for which "d2 > hi" stays false.
+__device__ __forceinline__ float pack_depth(float hi, uint32_t depth) {
+    return __uint_as_float(((__float_as_uint(hi) + 32u) & ~31u) | depth);
+}
+
+// Writes the MAC fields of record k: internal cells get (hi|depth, lo); a
+// leaf (count >= 1 bodies) is always summed directly: one body -> hi = -1 (it
+// passes as a point mass at its own position, which is its f32 centre of
+// mass exactly) and u.x = 1; several bodies -> hi = +inf (no point-mass
+// term) and u.x = count, summed body by body.
+__device__ __forceinline__ void store_mac_fields(CellRec* cell_r, uint32_t k, float fx, float fy,
+                                                 float gm, uint32_t depth, uint32_t leaf_count,
+                                                 double root_half, double theta) {
+    float lo = 0.f, hi;
+    uint32_t ux;
+    if (leaf_count) {
+        hi = leaf_count == 1u ? -1.0f : INFINITY;
+        ux = leaf_count;
+    } else {
+        const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(depth)), 2.0);
+        mac_band(width, theta, fx, fy, &lo, &hi);
+        ux = __float_as_uint(lo);
+    }
+    cell_r[k].f = make_float4(fx, fy, gm, pack_depth(hi, depth));
+    reinterpret_cast<uint32_t*>(&cell_r[k].u)[0] = ux;
+}
+
+// Writes a cell's f64 aggregates (centre of mass = weighted sums / mass, as
+// flat.rs:193-212) and its traversal record.
 __device__ __forceinline__ void store_cell_values(uint32_t k, double mass, double wx, double wy,
-                                                  uint32_t depth, double root_half,
-                                                  double4* cell_d, float4* cell_f) {
+                                                  uint32_t depth, uint32_t leaf_count,
+                                                  double root_half, double theta, float g,
+                                                  double4* cell_d, CellRec* cell_r) {
     const double com_x = __ddiv_rn(wx, mass);
     const double com_y = __ddiv_rn(wy, mass);
     cell_d[k] = make_double4(com_x, com_y, mass, 0.0);
-    const double half = __dmul_rn(root_half, pow2_neg(depth));
-    cell_f[k] = make_float4((float)com_x, (float)com_y, (float)mass, (float)__dmul_rn(half, 2.0));
+    store_mac_fields(cell_r, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass), depth,
+                     leaf_count, root_half, theta);
 }
 
 // Leaves (the last cell of each chain) sum their bodies in Morton order; the
@@ -654,11 +719,11 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
                                                    const uint32_t* __restrict__ chunk_sim,
                                                    uint32_t npos, const uint32_t* __restrict__ base,
                                                    const float4* __restrict__ sbody,
-                                                   const uint4* __restrict__ cell_u,
+                                                   CellRec* cell_r,
+                                                   const uint32_t* __restrict__ cell_end,
                                                    const uint4* __restrict__ cell_child,
                                                    const uint32_t* __restrict__ cell_parent,
-                                                   uint32_t* cell_counter, double4* cell_d,
-                                                   float4* cell_f) {
+                                                   uint32_t* cell_counter, double4* cell_d) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npos) return;
     const uint32_t s = chunk_sim[p >> 5];
@@ -669,18 +734,21 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
     const uint32_t c = base[p + 1] - k0;
     if (c == 0) return;
     const double root_half = simout[s].half;
+    const double theta = sd.theta;
+    const float g = sd.g_f;
     uint32_t k = k0 + c - 1u;
     {
-        const uint4 u = cell_u[k];
+        const uint32_t start = cell_r[k].u.z, end = cell_end[k];
         double mass = 0.0, wx = 0.0, wy = 0.0;
-        for (uint32_t q = u.x; q < u.y; ++q) {
+        for (uint32_t q = start; q < end; ++q) {
             const float4 b = sbody[q];
             const double m = (double)b.z;
             mass = __dadd_rn(mass, m);
             wx = __dadd_rn(wx, __dmul_rn(m, (double)b.x));
             wy = __dadd_rn(wy, __dmul_rn(m, (double)b.y));
         }
-        store_cell_values(k, mass, wx, wy, u.w, root_half, cell_d, cell_f);
+        store_cell_values(k, mass, wx, wy, cell_r[k].u.w, end - start, root_half, theta, g,
+                          cell_d, cell_r);
     }
     while (true) {
         const uint32_t par = cell_parent[k];
@@ -702,9 +770,27 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
             wx = __dadd_rn(wx, __dmul_rn(cm, cxy.x));
             wy = __dadd_rn(wy, __dmul_rn(cm, cxy.y));
         }
-        store_cell_values(par, mass, wx, wy, cell_u[par].w, root_half, cell_d, cell_f);
+        store_cell_values(par, mass, wx, wy, cell_r[par].u.w, 0u, root_half, theta, g, cell_d,
+                          cell_r);
         k = par;
     }
+}
+
+// Recomputes G*m and the MAC band of every cell of one simulation from the
+// f64 aggregates, for a force pass whose theta or G differs from the rebuild's.
+__global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
+                              uint32_t sim, const uint32_t* __restrict__ base,
+                              const double4* __restrict__ cell_d, CellRec* cell_r) {
+    const SimDesc& sd = sims[sim];
+    const uint32_t cb = base[sd.off], ce = base[sd.off + sd.n];
+    const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ce) return;
+    const uint4 u = cell_r[k].u;
+    const float4 f = cell_r[k].f;
+    const double4 v = cell_d[k];
+    const bool leaf = u.y == k + 1u;
+    store_mac_fields(cell_r, k, f.x, f.y, __fmul_rn(sd.g_f, (float)v.z), u.w, leaf ? u.x : 0u,
+                     simout[sim].half, sd.theta);
 }
 
 // ============================================================ traverse ====
@@ -736,20 +822,50 @@ struct Acc {
 // and walks the union of its lanes' traversals in preorder using skip
 // pointers (first child = next cell, skip = next cell after the subtree).
 // Each lane keeps exactly its own decisions: lane L acts on a cell only if
-// L opened the cell's parent (mask held per depth in lane `depth`), so every
-// lane visits the cells of nbody/src/flat.rs:270-346 in the same order and
-// sums the same terms in the same order.  The MAC is decided in f32 unless
-// the f32 margin is inside a guard band, where it is re-decided in f64 from
-// the f64 centre of mass exactly as the reference computes it.
+// L opened the cell's parent (the opener mask of the current depth-d
+// ancestor lives in lane d-1; lane 31 holds the root's mask), so every lane
+// visits the cells of nbody/src/flat.rs:270-346 in the same order and sums
+// the same terms in the same order.
+//
+// One branch-free iteration per cell: a lane approximates (or, for a
+// one-body leaf, sums the body) iff it is active, the cell does not hold its
+// own body and d2 > hi; it opens iff the cell is internal and holds its body
+// or d2 < lo.  "Holds body p" is a preorder interval test on the leaf index
+// L_p of p: c <= L_p < skip(c).  Lanes with lo <= d2 <= hi decide in f64
+// from the f64 centre of mass exactly as the reference (rare); leaves of
+// several bodies sum them one by one (rare for bucket 1).
+// Exact f64 opening test of flat.rs:317-323 for a lane inside the guard
+// band; true = approximate.
+__device__ __noinline__ bool exact_mac(const double4* __restrict__ cell_d, uint32_t c, float tx,
+                                       float ty, double root_half, uint32_t depth,
+                                       double theta) {
+    const double2 com = *reinterpret_cast<const double2*>(cell_d + c);
+    const double ddx = __dsub_rn(com.x, (double)tx);
+    const double ddy = __dsub_rn(com.y, (double)ty);
+    const double dist = hypot(ddx, ddy);
+    const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(depth)), 2.0);
+    return dist > 0.0 && __ddiv_rn(width, dist) < theta;
+}
+
+#ifndef GBH_TRAVERSE_WARPS
+#define GBH_TRAVERSE_WARPS 8
+#endif
+#ifndef GBH_TRAVERSE_MIN_BLOCKS
+#define GBH_TRAVERSE_MIN_BLOCKS 1
+#endif
+#ifndef GBH_TRAVERSE_PREFETCH
+#define GBH_TRAVERSE_PREFETCH 0
+#endif
+constexpr uint32_t kTravWarps = GBH_TRAVERSE_WARPS;
+
 template <bool COMP, bool POT, bool STATS>
-__global__ void __launch_bounds__(256) k_traverse(
+__global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_traverse(
     const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
     const uint32_t* __restrict__ chunk_sim, uint32_t nchunks, const float4* __restrict__ sbody,
-    const float4* __restrict__ cell_f, const uint4* __restrict__ cell_u,
-    const double4* __restrict__ cell_d, const uint32_t* __restrict__ base,
-    unsigned long long* stats, uint32_t* err) {
+    const CellRec* __restrict__ cells, const double4* __restrict__ cell_d,
+    const uint32_t* __restrict__ base, unsigned long long* stats) {
     const uint32_t lane = lane_id();
-    const uint32_t chunk = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const uint32_t chunk = blockIdx.x * kTravWarps + (threadIdx.x >> 5);
     if (chunk >= nchunks) return;
     const uint32_t s = chunk_sim[chunk];
     if (s == kNone) return;
@@ -759,100 +875,96 @@ __global__ void __launch_bounds__(256) k_traverse(
     const bool valid = p < end_pos;
     const float4 me = valid ? sbody[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float tx = me.x, ty = me.y;
+    const uint32_t leaf_p = valid ? base[p + 1] - 1u : kNone;  // preorder index of p's leaf
     const float eps2 = sd.eps_f * sd.eps_f;
     const float g = sd.g_f;
-    const float inv_theta = sd.inv_theta_f;
-    const double theta = sd.theta;
-    const double root_half = simout[s].half;
     const uint32_t valid_mask = __ballot_sync(kFull, valid);
     uint32_t c = base[sd.off];
     const uint32_t cend = base[end_pos];
-    uint32_t om = 0;  // lane d: mask of lanes that opened the current depth-d ancestor
+    uint32_t om = lane == 31u ? valid_mask : 0u;
     Acc<COMP> acc;
     float phi = 0.f;
-    uint32_t n_visit = 0, n_approx = 0, n_direct = 0, n_exact = 0;
+    uint32_t n_visit = 0, n_approx = 0, n_direct = 0, n_exact = 0, n_iter = 0;
 
-    auto interact = [&](float dx, float dy, float m) {
-        const float r2 = dx * dx + dy * dy + eps2;
-        const float inv_r = rsqrtf(r2);
-        const float scale = g * m * inv_r * inv_r * inv_r;
+    auto interact = [&](float dx, float dy, float d2, float gm) {
+        const float inv_r = rsqrtf(d2 + eps2);
+        const float scale = gm * inv_r * inv_r * inv_r;
         acc.add(dx * scale, dy * scale);
-        if (POT) phi -= g * m * inv_r;
+        if (POT) phi -= gm * inv_r;
     };
 
-    while (c < cend) {
-        const uint4 u = cell_u[c];
-        const float4 f = cell_f[c];
-        const uint32_t depth = u.w;
-        const uint32_t M = depth == 0 ? valid_mask : __shfl_sync(kFull, om, (depth - 1u) & 31u);
+    float4 f = cells[c].f;  // com_x, com_y, G*m, hi|depth
+    uint4 u = cells[c].u;   // lo | leaf count, skip, start, depth
+    while (true) {
+        const uint32_t hi_bits = __float_as_uint(f.w);
+        const uint32_t depth = hi_bits & 31u;
+        const uint32_t skip = u.y;
+#if GBH_TRAVERSE_PREFETCH
+        // the successor is c+1 whenever a lane opens c or c is a leaf
+        const CellRec* nxt = cells + min(c + 1u, cend - 1u);
+        const float4 nf = nxt->f;
+        const uint4 nu = nxt->u;
+#endif
+        const uint32_t M = __shfl_sync(kFull, om, (depth + 31u) & 31u);
         const bool active = (M >> lane) & 1u;
-        if (STATS && active) ++n_visit;
-        if (u.z <= c) {
-            set_err(err, kErrTraversal);
-            break;
+        const bool leaf = skip == c + 1u;
+        const bool holds_p = (leaf_p - c) < (skip - c);
+        const float dx = f.x - tx, dy = f.y - ty;
+        const float d2 = dx * dx + dy * dy;
+        bool approx = active && !holds_p && d2 > f.w;
+        bool open = active && !leaf && (holds_p || d2 < __uint_as_float(u.x));
+        const bool undecided = active && !leaf && !approx && !open;
+        if (STATS) {
+            n_visit += active;
+            n_iter += 1;
         }
-        if (u.z == c + 1u) {
-            // leaf: always summed directly (flat.rs:297-315), self excluded
-            if (u.y - u.x == 1u) {
-                if (active && u.x != p) {
-                    interact(f.x - tx, f.y - ty, f.z);
-                    if (STATS) ++n_direct;
-                }
-            } else {
-                for (uint32_t q = u.x; q < u.y; ++q) {
-                    const float4 b = sbody[q];
-                    if (active && q != p) {
-                        interact(b.x - tx, b.y - ty, b.z);
-                        if (STATS) ++n_direct;
-                    }
-                }
+        if (__any_sync(kFull, undecided)) {
+            if (undecided) {
+                approx = exact_mac(cell_d, c, tx, ty, simout[s].half, depth, sd.theta);
+                open = !approx;
+                if (STATS) ++n_exact;
             }
-            c = u.z;
-            continue;
         }
-        bool open = false;
-        if (active) {
-            const bool contains = p >= u.x && p < u.y;
-            const float dx = f.x - tx, dy = f.y - ty;
-            if (contains || !(theta > 0.0)) {
-                open = true;
-            } else {
-                const float d2 = dx * dx + dy * dy;
-                const float crit = f.w * inv_theta;
-                const float crit2 = crit * crit;
-                const float a = 2.4e-7f * (fabsf(f.x) + fabsf(f.y) + fabsf(dx) + fabsf(dy));
-                const float guard = 1e-4f * crit2 + 4.f * crit * a + 4.f * a * a;
-                const float margin = d2 - crit2;
-                bool approx;
-                if (margin > guard) {
-                    approx = true;
-                } else if (margin < -guard) {
-                    approx = false;
-                } else {
-                    // f64 MAC exactly as flat.rs:317-323
-                    const double2 com = *reinterpret_cast<const double2*>(cell_d + c);
-                    const double ddx = __dsub_rn(com.x, (double)tx);
-                    const double ddy = __dsub_rn(com.y, (double)ty);
-                    const double dist = hypot(ddx, ddy);
-                    const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(depth)), 2.0);
-                    approx = dist > 0.0 && __ddiv_rn(width, dist) < theta;
-                    if (STATS) ++n_exact;
-                }
-                if (approx) {
-                    interact(dx, dy, f.z);
-                    if (STATS) ++n_approx;
-                } else {
-                    open = true;
+        if (__any_sync(kFull, approx)) {
+            // point-mass term, branch-free within the warp: scale 0 for lanes
+            // that do not approximate this cell
+            const float inv_r = rsqrtf(d2 + eps2);
+            const float scale = approx ? f.z * inv_r * inv_r * inv_r : 0.f;
+            acc.add(dx * scale, dy * scale);
+            if (POT) phi -= approx ? f.z * inv_r : 0.f;
+            if (STATS) {
+                n_approx += approx && !leaf;
+                n_direct += approx && leaf;
+            }
+        }
+        if (leaf && (hi_bits & 0x7f800000u) == 0x7f800000u) {
+            // leaf of several bodies: each summed directly, self excluded (flat.rs:297-315)
+            for (uint32_t q = u.z; q < u.z + u.x; ++q) {
+                const float4 b = sbody[q];
+                if (active && q != p) {
+                    const float bx = b.x - tx, by = b.y - ty;
+                    interact(bx, by, bx * bx + by * by, __fmul_rn(g, b.z));
+                    if (STATS) ++n_direct;
                 }
             }
         }
         const uint32_t O = __ballot_sync(kFull, open);
-        if (O) {
-            if (lane == depth) om = O;
-            c = c + 1u;
+        if (lane == depth) om = O;
+        const uint32_t next = O ? c + 1u : max(skip, c + 1u);
+        if (next >= cend) break;
+#if GBH_TRAVERSE_PREFETCH
+        if (next == c + 1u) {
+            f = nf;
+            u = nu;
         } else {
-            c = u.z;
+            f = cells[next].f;
+            u = cells[next].u;
         }
+#else
+        f = cells[next].f;
+        u = cells[next].u;
+#endif
+        c = next;
     }
     if (valid) {
         const uint32_t idx = __float_as_uint(me.w);
@@ -872,6 +984,7 @@ __global__ void __launch_bounds__(256) k_traverse(
             atomicAdd(&stats[1], (unsigned long long)n_approx);
             atomicAdd(&stats[2], (unsigned long long)n_direct);
             atomicAdd(&stats[3], (unsigned long long)n_exact);
+            atomicAdd(&stats[4], (unsigned long long)n_iter);
         }
     }
 }
@@ -1000,7 +1113,9 @@ __global__ void __launch_bounds__(256) k_traverse_packed(
 // with the same f64 steps as child_bounds (nbody/src/flat.rs:96-103).
 __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
                                uint32_t sim, const uint32_t* __restrict__ codes,
-                               const uint32_t* __restrict__ base, const uint4* __restrict__ cell_u,
+                               const uint32_t* __restrict__ base,
+                               const CellRec* __restrict__ cell_r,
+                               const uint32_t* __restrict__ cell_end,
                                const uint4* __restrict__ cell_child,
                                const double4* __restrict__ cell_d, GpuCell* out) {
     const SimDesc& sd = sims[sim];
@@ -1008,9 +1123,9 @@ __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* _
     const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ce) return;
     const SimOut so = simout[sim];
-    const uint4 u = cell_u[k];
-    const uint32_t start = u.x - sd.off;
-    const uint32_t code = codes[u.x];
+    const uint4 u = cell_r[k].u;
+    const uint32_t start = u.z - sd.off;
+    const uint32_t code = codes[u.z];
     double cx = so.cx, cy = so.cy, half = so.half;
     for (uint32_t level = 0; level < u.w; ++level) {
         const uint32_t q = (code >> (30u - 2u * level)) & 3u;
@@ -1031,7 +1146,7 @@ __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* _
     c.com[2] = 0.f;
     c.com[3] = 0.f;
     c.range_depth[0] = start;
-    c.range_depth[1] = u.y - sd.off;
+    c.range_depth[1] = cell_end[k] - sd.off;
     c.range_depth[2] = u.w;
     c.range_depth[3] = 0u;
     c.children[0] = ch.x == kNone ? kNone : ch.x - cb;
@@ -1167,26 +1282,33 @@ cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
 
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
     k_cells<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
-                                                 b.keys_a, b.base, b.cell_u, b.cell_child,
-                                                 b.cell_parent, b.cell_counter, b.err);
+                                                 b.keys_a, b.base, b.cell_r, b.cell_end,
+                                                 b.cell_child, b.cell_parent, b.cell_counter,
+                                                 b.err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
     k_aggregate<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.npos,
-                                                     b.base, b.sbody, b.cell_u, b.cell_child,
-                                                     b.cell_parent, b.cell_counter, b.cell_d,
-                                                     b.cell_f);
+                                                     b.base, b.sbody, b.cell_r, b.cell_end,
+                                                     b.cell_child, b.cell_parent, b.cell_counter,
+                                                     b.cell_d);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {
+    k_refresh_mac<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(b.sims, b.simout, sim, b.base,
+                                                                 b.cell_d, b.cell_r);
     return cudaGetLastError();
 }
 
 cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
                             cudaStream_t s) {
-    const uint32_t blocks = (b.nchunks + 7) / 8;
-#define GBH_TRAVERSE(C, P, S)                                                                  \
-    k_traverse<C, P, S><<<blocks, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.nchunks,      \
-                                               b.sbody, b.cell_f, b.cell_u, b.cell_d, b.base, \
-                                               b.force_stats, b.err)
+    const uint32_t blocks = (b.nchunks + kTravWarps - 1) / kTravWarps;
+#define GBH_TRAVERSE(C, P, S)                                                                   \
+    k_traverse<C, P, S><<<blocks, kTravWarps * 32, 0, s>>>(b.sims, b.simout, b.chunk_sim,      \
+                                                           b.nchunks, b.sbody, b.cell_r,       \
+                                                           b.cell_d, b.base, b.force_stats)
     if (stats) {
         if (compensated) {
             if (potential) GBH_TRAVERSE(true, true, true); else GBH_TRAVERSE(true, false, true);
@@ -1208,7 +1330,8 @@ cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries
                           GpuCell* cells, cudaStream_t s) {
     if (cells)
         k_export_cells<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
-            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_u, b.cell_child, b.cell_d, cells);
+            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_r, b.cell_end, b.cell_child, b.cell_d,
+            cells);
     if (entries || bodies)
         k_export_entries<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, sim, b.keys_a, b.sbody,
                                                              entries, bodies);

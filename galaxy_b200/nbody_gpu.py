@@ -451,7 +451,8 @@ class ParallelTreeRuntime:
         s = BhForceStats()
         check(_lib.load().galaxy_bh_force_stats(gpu.handle, tree.handle, C.byref(s)))
         return {"visited_nodes": s.visited_nodes, "approximated_cells": s.approximated_cells,
-                "direct_terms": s.direct_terms, "exact_mac_fallbacks": s.exact_mac_fallbacks}
+                "direct_terms": s.direct_terms, "exact_mac_fallbacks": s.exact_mac_fallbacks,
+                "warp_iterations": s.warp_iterations}
 
     def step(self, gpu: NbodyGpu, evolving: EvolvingState, tree: ParallelGpuTree,
              config: Config, dt_myr: float, steps: int) -> None:

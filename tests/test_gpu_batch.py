@@ -1,0 +1,69 @@
+"""Batched engine: a member's result is the same alone and in the mix.
+
+Each simulation advanced inside a batch of uneven sizes, scenarios and
+configs must end bit-identical (state and accelerations) to the same
+simulation advanced alone through the plain path — per-simulation results
+never depend on the batch composition.
+"""
+import numpy as np
+import pytest
+
+from galaxy_b200 import scenarios
+from galaxy_b200.batch import Batch
+from galaxy_b200.nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime
+
+pytestmark = pytest.mark.gpu
+
+MEMBERS = [
+    ("exponential_disc", 1500, 11, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)),
+    ("cold_disc", 40000, 12, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=4)),
+    ("binary_encounter", 4097, 13, Config(theta=0.3, softening_kpc=0.005, g=1.0, bucket=1)),
+    ("exponential_disc", 70001, 14, Config(theta=0.7, softening_kpc=0.01, g=1.0, bucket=8)),
+    ("cold_disc", 33, 15, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=16)),
+]
+DTS = [1e-3, 5e-4, 1e-3, 2e-3, 1e-3]
+STEPS = 4
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    return NbodyGpu("0")
+
+
+def _alone(gpu, bodies, cfg, dt):
+    rt = ParallelTreeRuntime(gpu)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    rt.step(gpu, ev, tree, cfg, dt, STEPS)
+    return (gpu.read_evolving_state_records(ev)[0], gpu.read_evolving_accelerations_f32(ev)[0])
+
+
+def test_batch_members_equal_alone(gpu):
+    bodies = [scenarios.make(name, n, seed) for name, n, seed, _ in MEMBERS]
+    states = [gpu.create_evolving_state(b)[0] for b in bodies]
+    batch = Batch(gpu, states, [m[3] for m in MEMBERS])
+    batch.solve()
+    batch.step(DTS, STEPS)
+    for k, (b, (_, _, _, cfg), dt) in enumerate(zip(bodies, MEMBERS, DTS)):
+        want_state, want_acc = _alone(gpu, b, cfg, dt)
+        got_state = gpu.read_evolving_state_records(states[k])[0]
+        got_acc = gpu.read_evolving_accelerations_f32(states[k])[0]
+        assert got_state.tobytes() == want_state.tobytes(), f"member {k} state"
+        assert np.array_equal(got_acc, want_acc), f"member {k} accelerations"
+
+
+def test_batch_solve_matches_plain_force(gpu):
+    bodies = [scenarios.make(name, n, seed) for name, n, seed, _ in MEMBERS]
+    states = [gpu.create_evolving_state(b)[0] for b in bodies]
+    batch = Batch(gpu, states, [m[3] for m in MEMBERS])
+    batch.solve()
+    rt = ParallelTreeRuntime(gpu)
+    for k, (b, (_, _, _, cfg)) in enumerate(zip(bodies, MEMBERS)):
+        ev, _ = gpu.create_evolving_state(b)
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        assert np.array_equal(gpu.read_evolving_accelerations_f32(states[k])[0],
+                              gpu.read_evolving_accelerations_f32(ev)[0])
