@@ -317,6 +317,19 @@ def run_engine(args, world, rank, local, pg):
         e2e_ms = float(t.item())
     e2e_value = world * N_BODIES * e2e_steps / (e2e_ms * 1e-3)
 
+    tree.close()
+    ev.close()
+    batched = None
+    if not args.no_batched:
+        batched = run_batched_leg(gpu, steps=min(args.steps, 20), warmup=args.warmup)
+        if pg:
+            t = torch.tensor([batched["ms_per_step"]], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            batched["value"] = world * batched["bodies"] / (float(t.item()) * 1e-3)
+    served = None
+    if not args.no_served:
+        served = run_served_leg(gpu, capacity=(batched or {}).get("value", value / world)
+                                / max(world, 1))
     if rank != 0:
         if pg:
             pg.barrier()
@@ -356,6 +369,8 @@ def run_engine(args, world, rank, local, pg):
                        "galaxy_bh_read_state to pinned host (C ABI)",
                 "wall_s": e2e_wall},
         "cpu_baseline": cpu,
+        "batched": batched,
+        "served": served,
         "clocks": clk,
         "gpu_launches": 10 * args.steps + 1,
         "gpu": gpu.info().get("name"),
@@ -364,6 +379,139 @@ def run_engine(args, world, rank, local, pg):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps: int = 5,
+                    plain_sims: int | None = None) -> dict:
+    """Mixed workload: `count` independent simulations, N log-uniform in
+    [2^10, 2^18], scenarios uniform over the three, per-simulation seeds,
+    eps 0.01, theta 0.5, dt 1e-3.  Batched: one launch per stage for all of
+    them.  Plain: each simulation alone through the plain path, one after
+    another (the same engine, tree per simulation)."""
+    import torch
+
+    from galaxy_b200 import scenarios
+    from galaxy_b200.batch import Batch
+    from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
+    plan = scenarios.mixed_batch(count, 10, 18, seed=2024)
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    states = []
+    for name, n, seed in plan:
+        states.append(gpu.create_evolving_state_records(
+            bodies_to_state(scenarios.make(name, n, seed, eps=0.01)))[0])
+    total = sum(s.count for s in states)
+    stream = torch.cuda.ExternalStream(gpu.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    batch = Batch(gpu, states, [cfg] * len(states))
+    batch.solve()
+    batch.step(1e-3, max(warmup, 3))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.step(1e-3, steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    b_ms = e0.elapsed_time(e1)
+    arena = batch.arena_bytes()
+    batch.close()
+    # plain path, simulation after simulation (a prefix of the plan when
+    # plain_sims is set; the rate is per body-step either way)
+    rt = ParallelTreeRuntime(gpu)
+    sims = states if plain_sims is None else states[:plain_sims]
+    trees = []
+    for s in sims:
+        t = rt.create_tree(gpu, s, cfg)
+        rt.rebuild(gpu, s, t, cfg)
+        rt.force(gpu, s, t, cfg)
+        rt.step(gpu, s, t, cfg, 1e-3, 1)
+        trees.append(t)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for s, t in zip(sims, trees):
+        rt.step(gpu, s, t, cfg, 1e-3, plain_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    p_ms = e0.elapsed_time(e1)
+    p_bodies = sum(s.count for s in sims)
+    for t in trees:
+        t.close()
+    for s in states:
+        s.close()
+    batched = total * steps / (b_ms * 1e-3)
+    plain = p_bodies * plain_steps / (p_ms * 1e-3)
+    return {"workload": f"{count} sims, N log-uniform [2^10, 2^18], mixed scenarios, "
+                        "eps 0.01, theta 0.5, bucket 1, dt 1e-3",
+            "bodies": total, "steps": steps, "ms_per_step": b_ms / steps,
+            "value": batched, "unit": METRIC, "arena_bytes": arena,
+            "plain_serial": {"value": plain, "steps": plain_steps, "sims": len(sims),
+                             "ms_per_step": p_ms / plain_steps},
+            "speedup_vs_plain": batched / plain}
+
+
+def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: float = 150.0,
+                   deadline: float = 120.0) -> dict:
+    """Served workload: Poisson arrivals, N log-uniform [2^12, 2^22], steps
+    log-uniform [10, 1000], scenario uniform, theta 0.5, eps 0.01, dt 1e-3,
+    admitted against a 150 GB budget and continuously batched; each request
+    brings its initial conditions (generated before the clock starts).
+
+    Latency: arrivals at 60% of the measured batched capacity for
+    `duration` s (the specified 200/s offers ~50x more work than one GPU
+    serves; its load factor is reported) -> p50/p99 time-to-result.
+    Throughput: the specified 200/s stream for 0.2 s (a saturating burst of
+    ~40 requests) served with continuous batching, against the same requests
+    run one after another through the plain path (both include state upload,
+    tree allocation, boundary solve and all steps)."""
+    import torch
+
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
+    from galaxy_b200.serve import GpuEngineOps, Server, poisson_requests
+    mean_work = 605_000 * 215.0  # E[N] * E[steps] of the distributions above
+    rate = max(0.2, 0.6 * capacity / mean_work)
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+
+    def bodies(r):
+        return scenarios.make(r.scenario, r.n, r.seed, eps=0.01)
+
+    def with_inputs(reqs):
+        for r in reqs:
+            r.bodies = bodies(r)
+        return reqs
+
+    budget = int(budget_gb * 2 ** 30)
+    reqs = with_inputs(poisson_requests(rate, duration, seed=11))
+    out = Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16).run(reqs,
+                                                                           deadline=deadline)
+    for r in reqs:
+        r.bodies = None
+    burst = with_inputs(poisson_requests(200.0, 0.2, seed=12))
+    sat = Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16).run(burst,
+                                                                           deadline=deadline)
+    torch.cuda.synchronize()
+    rt = ParallelTreeRuntime(gpu)
+    t0 = time.perf_counter()
+    ps = 0
+    for r in burst:
+        ev, _ = gpu.create_evolving_state_records(bodies_to_state(r.bodies))
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        rt.step(gpu, ev, tree, cfg, r.dt, r.steps)
+        tree.close()
+        ev.close()
+        ps += r.n * r.steps
+    plain = ps / (time.perf_counter() - t0)
+    return {
+        "workload": "Poisson arrivals, N log-uniform [2^12,2^22], steps log-uniform [10,1000], "
+                    "mixed scenarios, theta 0.5, eps 0.01, dt 1e-3, 150 GB budget",
+        "latency": dict(out, rate_per_s=rate, arrival_window_s=duration),
+        "specified_rate_per_s": 200.0,
+        "specified_load_factor": 200.0 * mean_work / capacity,
+        "saturated": dict(sat, rate_per_s=200.0, arrival_window_s=0.2),
+        "plain_serial": {"particle_steps_per_s": plain, "requests": len(burst),
+                         "includes": "state upload, tree allocation, boundary solve, steps"},
+        "speedup_vs_plain": sat["particle_steps_per_s"] / plain if plain else None}
 
 
 def tree_cells(gpu, rt, tree) -> int:
@@ -383,6 +531,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the mixed-size batched workload leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served workload leg")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -1169,7 +1169,10 @@ extern "C" int galaxy_bh_batch_step(bh_device* dev, bh_batch* batch, const doubl
     int rc = enter(dev);
     if (rc) return rc;
     if (!batch || !dts || batch->dev != dev) return set_error(BH_INVALID_ARG, "null argument");
-    if (!batch->solved) return set_error(BH_INVALID_ARG, "batch step requires batch_solve first");
+    // Each member's acceleration buffer must already hold its boundary
+    // acceleration (from galaxy_bh_batch_solve, galaxy_bh_force, or earlier
+    // steps of any batch or tree): a batch re-formed after members left can
+    // step at once.
     Batch* b = batch->batch;
     for (size_t s = 0; s < b->h_sims.size(); ++s) {
         float f = 0.f;

@@ -243,7 +243,10 @@ int galaxy_bh_batch_create(bh_device* dev, bh_state* const* states, const bh_con
 int galaxy_bh_batch_destroy(bh_batch* batch);
 /* rebuild + force for every member (the boundary solve). */
 int galaxy_bh_batch_solve(bh_device* dev, bh_batch* batch);
-/* nsteps fused KDK steps for every member, dts[i] per member. */
+/* nsteps fused KDK steps for every member, dts[i] per member.  Each member's
+ * acceleration buffer must hold its boundary acceleration (a batch_solve,
+ * force or earlier step of that state); no solve is needed when a batch is
+ * re-formed from states that were already stepping. */
 int galaxy_bh_batch_step(bh_device* dev, bh_batch* batch, const double* dts, uint32_t nsteps);
 int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
 /* Device bytes a batch of these sizes/configs would need (admission). */

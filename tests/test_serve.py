@@ -1,0 +1,146 @@
+"""Serving loop logic on the CPU with a fake engine (admission against the
+memory budget, FIFO order, rounds, completion accounting), and on the GPU:
+every served result equals the same request run alone through the plain
+path, bit for bit, while other requests join and leave around it."""
+import numpy as np
+import pytest
+
+from galaxy_b200.serve import EngineOps, Request, Server, poisson_requests
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-4)
+
+
+class FakeOps(EngineOps):
+    """Each body costs 100 bytes; a step costs 1 ns per body."""
+
+    def __init__(self, clock):
+        self.clock = clock
+        self.live = {}
+        self.peak_bytes = 0
+        self.admit_order = []
+        self.steps_done = {}
+
+    def footprint(self, counts):
+        return 100 * sum(counts)
+
+    def create(self, req):
+        self.live[req.rid] = req.n
+        self.admit_order.append(req.rid)
+        self.peak_bytes = max(self.peak_bytes, self.footprint(list(self.live.values())))
+        self.steps_done[req.rid] = 0
+        return req.rid
+
+    def make_batch(self, handles):
+        return list(handles)
+
+    def solve(self, batch):
+        pass
+
+    def step(self, batch, dts, steps):
+        for h in batch:
+            self.steps_done[h] += steps
+        self.clock.t += 1e-9 * steps * sum(self.live[h] for h in batch)
+
+    def result(self, handle):
+        return self.steps_done[handle]
+
+    def release(self, handle):
+        del self.live[handle]
+
+    def release_batch(self, batch):
+        pass
+
+
+def test_poisson_requests_distribution():
+    reqs = poisson_requests(200.0, 5.0, seed=3)
+    assert 800 < len(reqs) < 1200
+    ns = np.array([r.n for r in reqs])
+    steps = np.array([r.steps for r in reqs])
+    assert ns.min() >= 2 ** 12 and ns.max() <= 2 ** 22
+    assert steps.min() >= 10 and steps.max() <= 1000
+    arr = np.array([r.arrival for r in reqs])
+    assert (np.diff(arr) > 0).all() and arr[-1] < 5.0
+    # log-uniform: median near the geometric mean
+    assert 2 ** 16 < np.median(ns) < 2 ** 18
+
+
+def test_server_admits_within_budget_and_completes_everything():
+    clock = FakeClock()
+    ops = FakeOps(clock)
+    reqs = [Request(i, "cold_disc", n, i, s, arr) for i, (n, s, arr) in enumerate(
+        [(1000, 30, 0.0), (5000, 10, 0.0), (3000, 25, 1e-6), (8000, 40, 2e-6), (500, 5, 5e-5)])]
+    budget = 100 * 9500  # never all at once
+    srv = Server(ops, budget, round_steps=8, keep_results=True, clock=clock, sleep=clock.sleep)
+    out = srv.run(reqs)
+    assert out["completed"] == len(reqs)
+    assert ops.peak_bytes <= budget
+    assert ops.admit_order == sorted(ops.admit_order)  # FIFO admission
+    for r in reqs:
+        assert r.result == r.steps  # every request got exactly its steps
+        assert r.finished >= r.admitted >= r.arrival
+    assert out["p99_s"] >= out["p50_s"] > 0
+    assert out["particle_steps"] == sum(r.n * r.steps for r in reqs)
+
+
+def test_server_rejects_request_larger_than_budget():
+    clock = FakeClock()
+    srv = Server(FakeOps(clock), 100 * 10, clock=clock, sleep=clock.sleep)
+    with pytest.raises(ValueError, match="exceeds the budget"):
+        srv.run([Request(0, "cold_disc", 100, 1, 10, 0.0)])
+
+
+def test_server_deadline_stops_early():
+    clock = FakeClock()
+    ops = FakeOps(clock)
+    reqs = [Request(i, "cold_disc", 10 ** 6, i, 1000, 0.0) for i in range(3)]
+    srv = Server(ops, 10 ** 12, round_steps=10, clock=clock, sleep=clock.sleep)
+    out = srv.run(reqs, deadline=0.05)
+    assert out["completed"] < 3
+
+
+@pytest.mark.gpu
+def test_served_results_equal_alone():
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime
+    from galaxy_b200.serve import GpuEngineOps
+
+    gpu = NbodyGpu("0")
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+
+    def bodies(r):
+        return scenarios.make(r.scenario, r.n, r.seed, eps=0.01)
+
+    ops = GpuEngineOps(gpu, cfg, bodies)
+    clock = FakeClock()
+
+    class Timed(GpuEngineOps):
+        def step(self, batch, dts, steps):
+            super().step(batch, dts, steps)
+            clock.t += 1e-3 * steps
+
+    ops = Timed(gpu, cfg, bodies)
+    reqs = [Request(0, "exponential_disc", 20000, 3, 23, 0.0),
+            Request(1, "cold_disc", 5000, 4, 7, 0.0),
+            Request(2, "binary_encounter", 12000, 5, 15, 0.005),
+            Request(3, "cold_disc", 3000, 6, 40, 0.012)]
+    srv = Server(ops, 1 << 40, round_steps=4, keep_results=True, clock=clock, sleep=clock.sleep)
+    out = srv.run(reqs)
+    assert out["completed"] == 4 and srv.rounds > 4
+    rt = ParallelTreeRuntime(gpu)
+    for r in reqs:
+        ev, _ = gpu.create_evolving_state(bodies(r))
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        rt.step(gpu, ev, tree, cfg, r.dt, r.steps)
+        alone = gpu.read_evolving_state_records(ev)[0]
+        assert alone.tobytes() == r.result.tobytes(), f"request {r.rid}"
