@@ -263,6 +263,33 @@ def run_engine(args, world, rank, local, pg):
         pg.barrier()
     value = world * N_BODIES * args.steps / (ms * 1e-3)
 
+    # --- FP64 direct-sum error of the evolved state's forces, 4096 probes
+    probes = np.random.default_rng(4096).choice(N_BODIES, 4096, replace=False)
+    force_error = gpu.probe_error(ev, cfg, probes)
+    force_error["theta"] = THETA
+
+    # --- the same workload at the opening angle whose median FP64 error is
+    # <= 1e-3 (theta = 0.12 on this workload; monopole cells at theta 0.5
+    # give ~1.6e-2, inherent to the reference's MAC)
+    acc_cfg = Config(theta=0.12, softening_kpc=EPS, g=G, bucket=BUCKET, max_depth=48)
+    ev2, _ = gpu.create_evolving_state_records(s0)
+    tree2 = rt.create_tree(gpu, ev2, acc_cfg)
+    rt.rebuild(gpu, ev2, tree2, acc_cfg)
+    rt.force(gpu, ev2, tree2, acc_cfg)
+    rt.step(gpu, ev2, tree2, acc_cfg, DT, 2)
+    acc_steps = max(3, min(args.steps // 10, 10))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    rt.step(gpu, ev2, tree2, acc_cfg, DT, acc_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    acc_ms = e0.elapsed_time(e1) / acc_steps
+    accurate = {"theta": 0.12, "value": world * N_BODIES / (acc_ms * 1e-3), "unit": METRIC,
+                "ms_per_step": acc_ms, "steps": acc_steps,
+                "force_error": gpu.probe_error(ev2, acc_cfg, probes)}
+    tree2.close()
+    ev2.close()
+
     # --- per-stage device times (instrumented rebuild + force, same state)
     reps = 5
     stage = {"bounds": 0.0, "morton": 0.0, "radix": 0.0, "topology": 0.0, "aggregate": 0.0,
@@ -369,6 +396,8 @@ def run_engine(args, world, rank, local, pg):
                        "galaxy_bh_read_state to pinned host (C ABI)",
                 "wall_s": e2e_wall},
         "cpu_baseline": cpu,
+        "force_error": force_error,
+        "at_1e-3_force_error": accurate,
         "batched": batched,
         "served": served,
         "clocks": clk,

@@ -117,6 +117,7 @@ SIGNATURES = {
     "galaxy_bh_force_into": (C.c_int, [_P, _P, _P, _P, _P, _P, _U32, C.POINTER(BhStageTiming)]),
     "galaxy_bh_step": (C.c_int, [_P, _P, _P, C.POINTER(BhConfig), C.c_double, _U32]),
     "galaxy_bh_conservation": (C.c_int, [_P, _P, C.POINTER(C.c_double)]),
+    "galaxy_bh_direct_probes": (C.c_int, [_P, _P, C.POINTER(BhConfig), _P, _U32, _P]),
     "galaxy_bh_conservation_noalloc": (C.c_int, [_P, _P, _U32, _P, _P]),
     "galaxy_bh_batch_create": (C.c_int, [_P, _P, C.POINTER(BhConfig), _U32, _PP]),
     "galaxy_bh_batch_destroy": (C.c_int, [_P]),

@@ -73,11 +73,17 @@ struct bh_device {
     cudaDeviceProp prop{};
     int refs = 0;         // live states, trees and batches on this device
     bool closed = false;  // galaxy_bh_device_close was called
+    // One released batch arena kept for the next batch: a serving loop that
+    // re-forms its batch after every membership change reuses it instead of
+    // freeing and allocating gigabytes each time.
+    void* spare = nullptr;
+    size_t spare_bytes = 0;
 };
 
 static void device_free(bh_device* dev) {
     cudaSetDevice(dev->ordinal);
     cudaStreamSynchronize(dev->stream);
+    cudaFree(dev->spare);
     for (auto& ev : dev->ev) cudaEventDestroy(ev);
     cudaStreamDestroy(dev->stream);
     delete dev;
@@ -442,6 +448,31 @@ static int ensure_potential(bh_state* st) {
     return BH_OK;
 }
 
+extern "C" int galaxy_bh_direct_probes(bh_device* dev, bh_state* st, const bh_config* cfg,
+                                       const uint32_t* probes, uint32_t nprobes, double* out) {
+    int rc = enter(dev);
+    if (rc) return rc;
+    if (!st || !cfg || !probes || !out) return set_error(BH_INVALID_ARG, "null argument");
+    if ((rc = validate_config(cfg))) return rc;
+    if (nprobes == 0) return BH_OK;
+    for (uint32_t k = 0; k < nprobes; ++k)
+        if (probes[k] >= st->n) return set_error(BH_INVALID_ARG, "body index is out of range");
+    uint32_t* d_p = nullptr;
+    double* d_o = nullptr;
+    cudaError_t e = cudaMalloc(&d_p, 4ull * nprobes);
+    if (!e) e = cudaMalloc(&d_o, 16ull * nprobes);
+    if (!e) e = cudaMemcpyAsync(d_p, probes, 4ull * nprobes, cudaMemcpyHostToDevice, dev->stream);
+    if (!e)
+        e = launch_direct_probes(st->d_state, st->n, d_p, nprobes, cfg->softening, cfg->g, d_o,
+                                 dev->stream);
+    if (!e) e = cudaMemcpyAsync(out, d_o, 16ull * nprobes, cudaMemcpyDeviceToHost, dev->stream);
+    if (!e) e = cudaStreamSynchronize(dev->stream);
+    cudaFree(d_p);
+    cudaFree(d_o);
+    if (e) return cuda_fail(e, "direct probes");
+    return BH_OK;
+}
+
 extern "C" int galaxy_bh_conservation(bh_device* dev, bh_state* st, double out[10]) {
     int rc = enter(dev);
     if (rc) return rc;
@@ -494,10 +525,21 @@ struct Batch {
     // (single-simulation trees; batches keep their creation configs)
     double built_theta = NAN, built_g = NAN;
 
+    size_t arena_capacity = 0;  // bytes actually held (>= arena_bytes when reused)
+
     ~Batch() {
         for (auto& g : graphs)
             if (g) cudaGraphExecDestroy(g);
-        cudaFree(arena);
+        if (!arena) return;
+        // keep the larger of this arena and the device's spare
+        cudaStreamSynchronize(dev->stream);
+        if (arena_capacity > dev->spare_bytes) {
+            cudaFree(dev->spare);
+            dev->spare = arena;
+            dev->spare_bytes = arena_capacity;
+        } else {
+            cudaFree(arena);
+        }
     }
 };
 
@@ -527,11 +569,12 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Byte sizes of the arena regions, in carve order.
 struct ArenaPlan {
-    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_r, cell_end,
-        cell_d, cell_child, cell_parent, cell_counter, err, stats;
+    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_r, groups,
+        cell_end, cell_d, cell_child, cell_parent, cell_counter, err, stats;
     size_t total() const {
         return control + sims + simout + chunk + tiles + 2 * keys + 2 * vals + sbody + base +
-               cell_r + cell_end + cell_d + cell_child + cell_parent + cell_counter + err + stats;
+               cell_r + groups + cell_end + cell_d + cell_child + cell_parent + cell_counter +
+               err + stats;
     }
 };
 
@@ -549,6 +592,7 @@ static ArenaPlan plan_arena(const Layout& L, uint32_t nsims) {
     a.sbody = align256(16ull * L.npos);
     a.base = align256(4ull * (L.npos + 1));
     a.cell_r = align256(sizeof(CellRec) * L.cells);
+    a.groups = align256(4ull * sizeof(CellRec) * (L.cells + nsims));
     a.cell_end = align256(4ull * L.cells);
     a.cell_d = align256(32ull * L.cells);
     a.cell_child = align256(16ull * L.cells);
@@ -597,8 +641,22 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     b->nscan_tiles = L.nscan_tiles;
     b->cell_capacity = L.cells;
     b->arena_bytes = A.total();
-    cudaError_t e = cudaMalloc(&b->arena, b->arena_bytes);
+    cudaError_t e = cudaSuccess;
+    if (dev->spare && dev->spare_bytes >= b->arena_bytes) {
+        b->arena = dev->spare;  // reuse the released arena of an earlier batch
+        b->arena_capacity = dev->spare_bytes;
+        dev->spare = nullptr;
+        dev->spare_bytes = 0;
+    } else {
+        cudaStreamSynchronize(dev->stream);
+        cudaFree(dev->spare);  // too small: give its memory back first
+        dev->spare = nullptr;
+        dev->spare_bytes = 0;
+        e = cudaMalloc(&b->arena, b->arena_bytes);
+        b->arena_capacity = b->arena_bytes;
+    }
     if (e != cudaSuccess) {
+        b->arena = nullptr;
         delete b;
         return cuda_fail(e, "batch arena allocation");
     }
@@ -634,6 +692,7 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.sbody = (float4*)take(A.sbody);
     bb.base = (uint32_t*)take(A.base);
     bb.cell_r = (CellRec*)take(A.cell_r);
+    bb.groups = (CellRec*)take(A.groups);
     bb.cell_end = (uint32_t*)take(A.cell_end);
     bb.cell_d = (double4*)take(A.cell_d);
     bb.cell_child = (uint4*)take(A.cell_child);

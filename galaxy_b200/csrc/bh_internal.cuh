@@ -99,7 +99,9 @@ struct BatchBuffers {
     uint32_t* vals_b;
     float4* sbody;      // sorted (x, y, m, body index bits)
     uint32_t* base;     // npos + 1: first cell index of each position's chain
-    CellRec* cell_r;    // traversal records
+    CellRec* cell_r;    // per-cell records in preorder (build, export, refresh)
+    CellRec* groups;    // node groups: children of cell k at [4k, 4k+4); simulation s's
+                        // root at slot 0 of group cell_capacity + s (traversal)
     uint32_t* cell_end; // end position (build and export only)
     double4* cell_d;    // com_x, com_y, mass, 0 (f64)
     uint4* cell_child;  // children (global cell indices)
@@ -128,6 +130,10 @@ cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bo
                                    const GpuEntry* entries, const GpuCell* cells, uint32_t n,
                                    uint32_t ncells, float4* accel, uint32_t* err,
                                    cudaStream_t s);
+// FP64 direct accelerations of nprobes probe bodies (out: 2 doubles each).
+cudaError_t launch_direct_probes(const GpuEvolveState* state, uint32_t n, const uint32_t* probes,
+                                 uint32_t nprobes, double eps, double g, double* out,
+                                 cudaStream_t s);
 // FP64 conservation partial sums: out gets 9 doubles (see galaxy_bh_conservation).
 cudaError_t launch_conservation(const GpuEvolveState* state, const float* potential, uint32_t n,
                                 double* partials, uint32_t nblocks, double* out,

@@ -16,8 +16,9 @@
 //   k_cells       ranges, children, skip pointers of every cell
 //   k_aggregate   bottom-up f64 mass / centre of mass, identical arithmetic
 //                 and order to nbody/src/flat.rs:179-215
-//   k_traverse    warp-cooperative theta-MAC traversal (nbody/src/flat.rs:
-//                 270-346 per body), f32 forces, exact f64 MAC in the guard band
+//   k_traverse    lane-parallel theta-MAC walk over node groups with per-warp
+//                 interaction lists (nbody/src/flat.rs:270-346 decisions per
+//                 body), f32 forces, exact f64 MAC in the guard band
 //
 // The f64 expressions that must reproduce the reference bit for bit use the
 // explicit round-to-nearest intrinsics (__dadd_rn, __dmul_rn, ...), which
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
                                                const uint32_t* __restrict__ base, CellRec* cell_r,
                                                uint32_t* cell_end, uint4* cell_child,
                                                uint32_t* cell_parent, uint32_t* cell_counter,
-                                               uint32_t* err) {
+                                               CellRec* groups, uint32_t* err) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npos) return;
     const uint32_t s = chunk_sim[p >> 5];
@@ -597,7 +598,15 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
         from = group_end(sc, n, i, (uint32_t)d, from);
         ends[d - dmin] = from;
     }
-    if (dmin == 0) cell_parent[k0] = kNone;
+    const uint4 absent = make_uint4(0u, 0u, 0u, kNone);  // u.z == 0: no child in this slot
+    if (dmin == 0) {
+        cell_parent[k0] = kNone;
+        // the simulation's root group holds the root in slot 0 only
+        CellRec* rg = groups + 4ull * (capacity + s);
+        rg[1].u = absent;
+        rg[2].u = absent;
+        rg[3].u = absent;
+    }
     for (uint32_t d = dmin; d <= deepest; ++d) {
         const uint32_t k = k0 + (d - dmin);
         const uint32_t end = ends[d - dmin];
@@ -629,6 +638,8 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
                         cell_parent[child] = k;
                     else
                         set_err(err, kErrCapacity);
+                } else {
+                    groups[4ull * k + q].u = absent;
                 }
             }
         }
@@ -680,34 +691,72 @@ __device__ __forceinline__ float pack_depth(float hi, uint32_t depth) {
 // passes as a point mass at its own position, which is its f32 centre of
 // mass exactly) and u.x = 1; several bodies -> hi = +inf (no point-mass
 // term) and u.x = count, summed body by body.
-__device__ __forceinline__ void store_mac_fields(CellRec* cell_r, uint32_t k, float fx, float fy,
-                                                 float gm, uint32_t depth, uint32_t leaf_count,
-                                                 double root_half, double theta) {
+// Where a cell sits for the traversal: slot `quadrant` of its parent's node
+// group, or slot 0 of its simulation's root group (index capacity + sim).
+struct SlotRef {
+    uint32_t parent;      // kNone for a root
+    uint32_t quadrant;
+    uint32_t root_group;  // capacity + sim
+};
+
+__device__ __forceinline__ CellRec* slot_of(CellRec* groups, const SlotRef& r) {
+    return groups + (r.parent == kNone ? 4ull * r.root_group : 4ull * r.parent + r.quadrant);
+}
+
+// Writes the MAC fields of cell k into its preorder record and into its slot
+// of the parent's node group: internal cells get (hi|depth, lo); a leaf
+// (count >= 1 bodies) is always summed directly: one body -> hi = -1 (it
+// passes as a point mass at its own position, which is its f32 centre of
+// mass exactly); several bodies -> hi = +inf (no point-mass term), summed
+// body by body.  The slot's u = (lo | body count, start, body count, k or
+// kNone for a leaf).
+__device__ __forceinline__ void store_mac_fields(CellRec* cell_r, CellRec* groups, uint32_t k,
+                                                 float fx, float fy, float gm, uint32_t depth,
+                                                 uint32_t start, uint32_t count, bool leaf,
+                                                 const SlotRef& slot, double root_half,
+                                                 double theta) {
     float lo = 0.f, hi;
     uint32_t ux;
-    if (leaf_count) {
-        hi = leaf_count == 1u ? -1.0f : INFINITY;
-        ux = leaf_count;
+    if (leaf) {
+        hi = count == 1u ? -1.0f : INFINITY;
+        ux = count;
     } else {
         const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(depth)), 2.0);
         mac_band(width, theta, fx, fy, &lo, &hi);
         ux = __float_as_uint(lo);
     }
-    cell_r[k].f = make_float4(fx, fy, gm, pack_depth(hi, depth));
+    const float4 f = make_float4(fx, fy, gm, pack_depth(hi, depth));
+    cell_r[k].f = f;
     reinterpret_cast<uint32_t*>(&cell_r[k].u)[0] = ux;
+    CellRec* sl = slot_of(groups, slot);
+    sl->f = f;
+    sl->u = make_uint4(ux, start, count, leaf ? kNone : k);
 }
 
 // Writes a cell's f64 aggregates (centre of mass = weighted sums / mass, as
-// flat.rs:193-212) and its traversal record.
+// flat.rs:193-212) and its traversal records.
 __device__ __forceinline__ void store_cell_values(uint32_t k, double mass, double wx, double wy,
-                                                  uint32_t depth, uint32_t leaf_count,
+                                                  uint32_t depth, uint32_t start, uint32_t count,
+                                                  bool leaf, const SlotRef& slot,
                                                   double root_half, double theta, float g,
-                                                  double4* cell_d, CellRec* cell_r) {
+                                                  double4* cell_d, CellRec* cell_r,
+                                                  CellRec* groups) {
     const double com_x = __ddiv_rn(wx, mass);
     const double com_y = __ddiv_rn(wy, mass);
     cell_d[k] = make_double4(com_x, com_y, mass, 0.0);
-    store_mac_fields(cell_r, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass), depth,
-                     leaf_count, root_half, theta);
+    store_mac_fields(cell_r, groups, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass),
+                     depth, start, count, leaf, slot, root_half, theta);
+}
+
+// Slot of cell k given its parent: the quadrant is the 2-bit digit of the
+// cell's codes at the parent's depth.
+__device__ __forceinline__ SlotRef slot_ref(uint32_t parent, uint32_t depth, uint32_t start_code,
+                                            uint32_t root_group) {
+    SlotRef r;
+    r.parent = parent;
+    r.quadrant = depth ? (start_code >> (32u - 2u * depth)) & 3u : 0u;
+    r.root_group = root_group;
+    return r;
 }
 
 // Leaves (the last cell of each chain) sum their bodies in Morton order; the
@@ -719,11 +768,13 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
                                                    const uint32_t* __restrict__ chunk_sim,
                                                    uint32_t npos, const uint32_t* __restrict__ base,
                                                    const float4* __restrict__ sbody,
-                                                   CellRec* cell_r,
+                                                   const uint32_t* __restrict__ codes,
+                                                   uint32_t capacity, CellRec* cell_r,
                                                    const uint32_t* __restrict__ cell_end,
                                                    const uint4* __restrict__ cell_child,
                                                    const uint32_t* __restrict__ cell_parent,
-                                                   uint32_t* cell_counter, double4* cell_d) {
+                                                   uint32_t* cell_counter, double4* cell_d,
+                                                   CellRec* groups) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npos) return;
     const uint32_t s = chunk_sim[p >> 5];
@@ -736,6 +787,7 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
     const double root_half = simout[s].half;
     const double theta = sd.theta;
     const float g = sd.g_f;
+    const uint32_t root_group = capacity + s;
     uint32_t k = k0 + c - 1u;
     {
         const uint32_t start = cell_r[k].u.z, end = cell_end[k];
@@ -747,8 +799,10 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
             wx = __dadd_rn(wx, __dmul_rn(m, (double)b.x));
             wy = __dadd_rn(wy, __dmul_rn(m, (double)b.y));
         }
-        store_cell_values(k, mass, wx, wy, cell_r[k].u.w, end - start, root_half, theta, g,
-                          cell_d, cell_r);
+        const uint32_t depth = cell_r[k].u.w;
+        store_cell_values(k, mass, wx, wy, depth, start, end - start, true,
+                          slot_ref(cell_parent[k], depth, codes[start], root_group), root_half,
+                          theta, g, cell_d, cell_r, groups);
     }
     while (true) {
         const uint32_t par = cell_parent[k];
@@ -770,8 +824,10 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
             wx = __dadd_rn(wx, __dmul_rn(cm, cxy.x));
             wy = __dadd_rn(wy, __dmul_rn(cm, cxy.y));
         }
-        store_cell_values(par, mass, wx, wy, cell_r[par].u.w, 0u, root_half, theta, g, cell_d,
-                          cell_r);
+        const uint32_t pstart = cell_r[par].u.z, pdepth = cell_r[par].u.w;
+        store_cell_values(par, mass, wx, wy, pdepth, pstart, cell_end[par] - pstart, false,
+                          slot_ref(cell_parent[par], pdepth, codes[pstart], root_group),
+                          root_half, theta, g, cell_d, cell_r, groups);
         k = par;
     }
 }
@@ -780,7 +836,11 @@ __global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ s
 // f64 aggregates, for a force pass whose theta or G differs from the rebuild's.
 __global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
                               uint32_t sim, const uint32_t* __restrict__ base,
-                              const double4* __restrict__ cell_d, CellRec* cell_r) {
+                              const uint32_t* __restrict__ codes, uint32_t capacity,
+                              const uint32_t* __restrict__ cell_end,
+                              const uint32_t* __restrict__ cell_parent,
+                              const double4* __restrict__ cell_d, CellRec* cell_r,
+                              CellRec* groups) {
     const SimDesc& sd = sims[sim];
     const uint32_t cb = base[sd.off], ce = base[sd.off + sd.n];
     const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
@@ -789,7 +849,10 @@ __global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __
     const float4 f = cell_r[k].f;
     const double4 v = cell_d[k];
     const bool leaf = u.y == k + 1u;
-    store_mac_fields(cell_r, k, f.x, f.y, __fmul_rn(sd.g_f, (float)v.z), u.w, leaf ? u.x : 0u,
+    const uint32_t start = u.z;
+    store_mac_fields(cell_r, groups, k, f.x, f.y, __fmul_rn(sd.g_f, (float)v.z), u.w, start,
+                     cell_end[k] - start, leaf,
+                     slot_ref(cell_parent[k], u.w, codes[start], capacity + sim),
                      simout[sim].half, sd.theta);
 }
 
@@ -818,22 +881,28 @@ struct Acc {
     __device__ __forceinline__ float fy() const { return COMP ? y + cy : y; }
 };
 
-// Warp-cooperative traversal.  A warp owns 32 consecutive Morton positions
-// and walks the union of its lanes' traversals in preorder using skip
-// pointers (first child = next cell, skip = next cell after the subtree).
-// Each lane keeps exactly its own decisions: lane L acts on a cell only if
-// L opened the cell's parent (the opener mask of the current depth-d
-// ancestor lives in lane d-1; lane 31 holds the root's mask), so every lane
-// visits the cells of nbody/src/flat.rs:270-346 in the same order and sums
-// the same terms in the same order.
-//
-// One branch-free iteration per cell: a lane approximates (or, for a
-// one-body leaf, sums the body) iff it is active, the cell does not hold its
-// own body and d2 > hi; it opens iff the cell is internal and holds its body
-// or d2 < lo.  "Holds body p" is a preorder interval test on the leaf index
-// L_p of p: c <= L_p < skip(c).  Lanes with lo <= d2 <= hi decide in f64
-// from the f64 centre of mass exactly as the reference (rare); leaves of
-// several bodies sum them one by one (rare for bucket 1).
+// Lane-parallel traversal with interaction lists.  A warp owns 32
+// consecutive Morton positions (its lanes).  Every lane keeps exactly its
+// own opening decisions of nbody/src/flat.rs:270-346, but the walk itself is
+// spread over the lanes: the warp pops up to 8 (node group, lane mask)
+// entries from a per-warp stack in shared memory, and lane 4i+q examines
+// slot q of popped entry i for all lanes of its mask at once, against the
+// bounding box of the warp's bodies:
+//   * the box's nearest point has d2 > hi: every lane of the mask
+//     approximates the cell (a lane whose own body the cell holds opens it);
+//   * the box's farthest corner has d2 < lo: every lane of the mask opens it;
+//   * otherwise the cell is mixed and the warp decides it lane by lane, as
+//     a single lane would (f64 test inside the guard band).
+// d2 is fma(dx, dx, dy*dy) in f32 with round-to-nearest, monotone in |dx|
+// and |dy|, and each lane's |dx|, |dy| lie between the box's nearest and
+// farthest distances, so a box decision is every lane's own decision.
+// Approximated cells and one-body leaves go to a per-warp interaction list
+// (centre of mass, G*m, mask of the lanes that take the term), which all
+// lanes sum with one branch-free masked term per entry; mixed cells add
+// their term directly and leaves of several bodies are summed body by body,
+// self excluded.  Only the order of a lane's terms differs from the
+// reference's depth-first order.
+
 // Exact f64 opening test of flat.rs:317-323 for a lane inside the guard
 // band; true = approximate.
 __device__ __noinline__ bool exact_mac(const double4* __restrict__ cell_d, uint32_t c, float tx,
@@ -847,125 +916,224 @@ __device__ __noinline__ bool exact_mac(const double4* __restrict__ cell_d, uint3
     return dist > 0.0 && __ddiv_rn(width, dist) < theta;
 }
 
+// Squared distance as the traversal computes it everywhere (monotone in |dx|
+// and |dy|; its rounding is covered by the guard band of mac_band).
+__device__ __forceinline__ float dist2(float dx, float dy) {
+    return __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+}
+
+// Lane mask of bits [a, b), 0 <= a <= b <= 32.
+__device__ __forceinline__ uint32_t bit_range(uint32_t a, uint32_t b) {
+    const uint32_t w = b - a;
+    return w >= 32u ? 0xffffffffu : (((1u << w) - 1u) << a);
+}
+
 #ifndef GBH_TRAVERSE_WARPS
 #define GBH_TRAVERSE_WARPS 8
 #endif
 #ifndef GBH_TRAVERSE_MIN_BLOCKS
-#define GBH_TRAVERSE_MIN_BLOCKS 1
-#endif
-#ifndef GBH_TRAVERSE_PREFETCH
-#define GBH_TRAVERSE_PREFETCH 0
+#define GBH_TRAVERSE_MIN_BLOCKS 4  // 64 registers: 32 warps per SM
 #endif
 constexpr uint32_t kTravWarps = GBH_TRAVERSE_WARPS;
+// Stack bound.  Each step pops the top <= 8 entries and pushes the opened
+// children groups (<= 32) in the order of their parents' stack positions, so
+// the stack stays sorted by depth with the deepest entries on top.  When
+// entries of depth d are pushed, every earlier entry of depth d has already
+// been popped (it sat above the depth d-1 parent), so at most 32 entries of
+// one depth are held at once.  Groups belong to the 16 internal depths 0..15
+// (Morton codes resolve 16 levels) or are a root group: 17 depths.
+constexpr uint32_t kTravStack = 17u * 32u;
+// Interaction list: flushed once it holds >= 32 entries; a step adds <= 32.
+constexpr uint32_t kTravList = 64u;
 
 template <bool COMP, bool POT, bool STATS>
 __global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_traverse(
     const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
     const uint32_t* __restrict__ chunk_sim, uint32_t nchunks, const float4* __restrict__ sbody,
-    const CellRec* __restrict__ cells, const double4* __restrict__ cell_d,
-    const uint32_t* __restrict__ base, unsigned long long* stats) {
+    const CellRec* __restrict__ groups, const double4* __restrict__ cell_d, uint32_t capacity,
+    unsigned long long* stats, uint32_t* err) {
+    __shared__ uint2 s_stack[kTravWarps][kTravStack];  // (node group, lane mask)
+    __shared__ float4 s_list[kTravWarps][kTravList];   // (com_x, com_y, G*m, lane mask bits)
     const uint32_t lane = lane_id();
-    const uint32_t chunk = blockIdx.x * kTravWarps + (threadIdx.x >> 5);
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t chunk = blockIdx.x * kTravWarps + warp;
     if (chunk >= nchunks) return;
     const uint32_t s = chunk_sim[chunk];
     if (s == kNone) return;
     const SimDesc& sd = sims[s];
-    const uint32_t p = chunk * kChunk + lane;
-    const uint32_t end_pos = sd.off + sd.n;
-    const bool valid = p < end_pos;
+    const uint32_t p0 = chunk * kChunk;
+    const uint32_t p = p0 + lane;
+    const bool valid = p < sd.off + sd.n;
     const float4 me = valid ? sbody[p] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float tx = me.x, ty = me.y;
-    const uint32_t leaf_p = valid ? base[p + 1] - 1u : kNone;  // preorder index of p's leaf
     const float eps2 = sd.eps_f * sd.eps_f;
     const float g = sd.g_f;
     const uint32_t valid_mask = __ballot_sync(kFull, valid);
-    uint32_t c = base[sd.off];
-    const uint32_t cend = base[end_pos];
-    uint32_t om = lane == 31u ? valid_mask : 0u;
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    float bx0 = valid ? tx : INFINITY, bx1 = valid ? tx : -INFINITY;
+    float by0 = valid ? ty : INFINITY, by1 = valid ? ty : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        bx0 = fminf(bx0, __shfl_xor_sync(kFull, bx0, o));
+        bx1 = fmaxf(bx1, __shfl_xor_sync(kFull, bx1, o));
+        by0 = fminf(by0, __shfl_xor_sync(kFull, by0, o));
+        by1 = fmaxf(by1, __shfl_xor_sync(kFull, by1, o));
+    }
+    uint2* stack = s_stack[warp];
+    float4* list = s_list[warp];
     Acc<COMP> acc;
     float phi = 0.f;
     uint32_t n_visit = 0, n_approx = 0, n_direct = 0, n_exact = 0, n_iter = 0;
 
-    auto interact = [&](float dx, float dy, float d2, float gm) {
+    // one point-mass term, scale 0 for lanes that do not take it
+    auto term = [&](float dx, float dy, float d2, float gm, bool take) {
         const float inv_r = rsqrtf(d2 + eps2);
-        const float scale = gm * inv_r * inv_r * inv_r;
+        const float scale = take ? gm * inv_r * inv_r * inv_r : 0.f;
         acc.add(dx * scale, dy * scale);
-        if (POT) phi -= gm * inv_r;
+        if (POT) phi -= take ? gm * inv_r : 0.f;
+    };
+    auto flush = [&](uint32_t count) {
+#pragma unroll 4
+        for (uint32_t i = 0; i < count; ++i) {
+            const float4 e = list[i];
+            const float dx = e.x - tx, dy = e.y - ty;
+            term(dx, dy, dist2(dx, dy), e.z, (__float_as_uint(e.w) >> lane) & 1u);
+        }
     };
 
-    float4 f = cells[c].f;  // com_x, com_y, G*m, hi|depth
-    uint4 u = cells[c].u;   // lo | leaf count, skip, start, depth
-    while (true) {
-        const uint32_t hi_bits = __float_as_uint(f.w);
-        const uint32_t depth = hi_bits & 31u;
-        const uint32_t skip = u.y;
-#if GBH_TRAVERSE_PREFETCH
-        // the successor is c+1 whenever a lane opens c or c is a leaf
-        const CellRec* nxt = cells + min(c + 1u, cend - 1u);
-        const float4 nf = nxt->f;
-        const uint4 nu = nxt->u;
-#endif
-        const uint32_t M = __shfl_sync(kFull, om, (depth + 31u) & 31u);
-        const bool active = (M >> lane) & 1u;
-        const bool leaf = skip == c + 1u;
-        const bool holds_p = (leaf_p - c) < (skip - c);
-        const float dx = f.x - tx, dy = f.y - ty;
-        const float d2 = dx * dx + dy * dy;
-        bool approx = active && !holds_p && d2 > f.w;
-        bool open = active && !leaf && (holds_p || d2 < __uint_as_float(u.x));
-        const bool undecided = active && !leaf && !approx && !open;
-        if (STATS) {
-            n_visit += active;
-            n_iter += 1;
+    if (lane == 0) stack[0] = make_uint2(capacity + s, valid_mask);
+    __syncwarp();
+    uint32_t len = 1, nlist = 0;
+    while (len > 0) {
+        const uint32_t ng = min(len, 8u);
+        const uint32_t gi = lane >> 2;
+        const bool have = gi < ng;
+        uint2 e = make_uint2(0u, 0u);
+        if (have) e = stack[len - ng + gi];
+        __syncwarp();
+        len -= ng;
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint4 u = make_uint4(0u, 0u, 0u, 0u);  // lo | count, start, count, cell (kNone: leaf)
+        if (have) {
+            const CellRec* r = groups + 4ull * e.x + (lane & 3u);
+            f = __ldg(&r->f);
+            u = __ldg(&r->u);
         }
-        if (__any_sync(kFull, undecided)) {
-            if (undecided) {
-                approx = exact_mac(cell_d, c, tx, ty, simout[s].half, depth, sd.theta);
-                open = !approx;
-                if (STATS) ++n_exact;
-            }
-        }
-        if (__any_sync(kFull, approx)) {
-            // point-mass term, branch-free within the warp: scale 0 for lanes
-            // that do not approximate this cell
-            const float inv_r = rsqrtf(d2 + eps2);
-            const float scale = approx ? f.z * inv_r * inv_r * inv_r : 0.f;
-            acc.add(dx * scale, dy * scale);
-            if (POT) phi -= approx ? f.z * inv_r : 0.f;
-            if (STATS) {
-                n_approx += approx && !leaf;
-                n_direct += approx && leaf;
-            }
-        }
-        if (leaf && (hi_bits & 0x7f800000u) == 0x7f800000u) {
-            // leaf of several bodies: each summed directly, self excluded (flat.rs:297-315)
-            for (uint32_t q = u.z; q < u.z + u.x; ++q) {
-                const float4 b = sbody[q];
-                if (active && q != p) {
-                    const float bx = b.x - tx, by = b.y - ty;
-                    interact(bx, by, bx * bx + by * by, __fmul_rn(g, b.z));
-                    if (STATS) ++n_direct;
+        const uint32_t A = e.y;
+        const bool present = u.z != 0u;
+        const bool leaf = u.w == kNone;
+        // lanes whose own body the cell holds: positions [start, start + count)
+        const uint32_t ha = max(u.y, p0), hb = min(u.y + u.z, p0 + 32u);
+        const uint32_t H = (present && ha < hb) ? bit_range(ha - p0, hb - p0) : 0u;
+        const uint32_t R = A & ~H;
+        uint32_t ap = 0u, op = 0u;
+        bool mixed = false, multi = false;
+        if (present) {
+            if (leaf) {
+                if (u.z == 1u)
+                    ap = R;
+                else
+                    multi = true;
+            } else {
+                op = A & H;
+                if (R) {
+                    const float nx = fmaxf(fmaxf(bx0 - f.x, f.x - bx1), 0.f);
+                    const float ny = fmaxf(fmaxf(by0 - f.y, f.y - by1), 0.f);
+                    const float fx = fmaxf(fabsf(f.x - bx0), fabsf(f.x - bx1));
+                    const float fy = fmaxf(fabsf(f.y - by0), fabsf(f.y - by1));
+                    if (dist2(nx, ny) > f.w)
+                        ap = R;
+                    else if (dist2(fx, fy) < __uint_as_float(u.x))
+                        op |= R;
+                    else
+                        mixed = true;
                 }
             }
+            if (STATS) {
+                n_visit += __popc(A);
+                if (leaf)
+                    n_direct += __popc(ap);
+                else
+                    n_approx += __popc(ap);
+            }
         }
-        const uint32_t O = __ballot_sync(kFull, open);
-        if (lane == depth) om = O;
-        const uint32_t next = O ? c + 1u : max(skip, c + 1u);
-        if (next >= cend) break;
-#if GBH_TRAVERSE_PREFETCH
-        if (next == c + 1u) {
-            f = nf;
-            u = nu;
-        } else {
-            f = cells[next].f;
-            u = cells[next].u;
+        if (STATS) ++n_iter;
+
+        // mixed cells: every lane of the mask decides for itself
+        uint32_t bm = __ballot_sync(kFull, mixed);
+        while (bm) {
+            const uint32_t src = __ffs(bm) - 1u;
+            bm &= bm - 1u;
+            const float cx = __shfl_sync(kFull, f.x, src);
+            const float cy = __shfl_sync(kFull, f.y, src);
+            const float gm = __shfl_sync(kFull, f.z, src);
+            const float hi = __shfl_sync(kFull, f.w, src);
+            const float lo = __uint_as_float(__shfl_sync(kFull, u.x, src));
+            const uint32_t start = __shfl_sync(kFull, u.y, src);
+            const uint32_t count = __shfl_sync(kFull, u.z, src);
+            const uint32_t k = __shfl_sync(kFull, u.w, src);
+            const uint32_t M = __shfl_sync(kFull, A, src);
+            const bool active = (M >> lane) & 1u;
+            const bool holds = (p - start) < count;
+            const float dx = cx - tx, dy = cy - ty;
+            const float d2 = dist2(dx, dy);
+            bool approx = active && !holds && d2 > hi;
+            bool open = active && (holds || d2 < lo);
+            const bool undecided = active && !approx && !open;
+            if (__any_sync(kFull, undecided)) {
+                if (undecided) {
+                    approx = exact_mac(cell_d, k, tx, ty, simout[s].half,
+                                       __float_as_uint(hi) & 31u, sd.theta);
+                    open = !approx;
+                    if (STATS) ++n_exact;
+                }
+            }
+            if (__any_sync(kFull, approx)) {
+                term(dx, dy, d2, gm, approx);
+                if (STATS) n_approx += approx;
+            }
+            const uint32_t O = __ballot_sync(kFull, open);
+            if (lane == src) op = O;
+            if (STATS) ++n_iter;
         }
-#else
-        f = cells[next].f;
-        u = cells[next].u;
-#endif
-        c = next;
+
+        // leaves of several bodies: each body summed directly, self excluded
+        uint32_t bl = __ballot_sync(kFull, multi);
+        while (bl) {
+            const uint32_t src = __ffs(bl) - 1u;
+            bl &= bl - 1u;
+            const uint32_t start = __shfl_sync(kFull, u.y, src);
+            const uint32_t count = __shfl_sync(kFull, u.z, src);
+            const uint32_t M = __shfl_sync(kFull, A, src);
+            const bool active = (M >> lane) & 1u;
+            for (uint32_t j = start; j < start + count; ++j) {
+                const float4 o = sbody[j];
+                const bool take = active && j != p;
+                const float dx = o.x - tx, dy = o.y - ty;
+                term(dx, dy, dist2(dx, dy), __fmul_rn(g, o.z), take);
+                if (STATS) n_direct += take;
+            }
+        }
+
+        // append the uniform terms, push the opened groups in lane order
+        const uint32_t la = __ballot_sync(kFull, ap != 0u);
+        if (ap) list[nlist + __popc(la & lanes_below)] = make_float4(f.x, f.y, f.z, __uint_as_float(ap));
+        nlist += __popc(la);
+        const uint32_t lp = __ballot_sync(kFull, op != 0u);
+        if (len + __popc(lp) > kTravStack) {  // unreachable by the bound above
+            if (lane == 0) set_err(err, kErrTraversal);
+            break;
+        }
+        if (op) stack[len + __popc(lp & lanes_below)] = make_uint2(u.w, op);
+        len += __popc(lp);
+        __syncwarp();
+        if (nlist >= 32u) {
+            flush(nlist);
+            nlist = 0;
+            __syncwarp();
+        }
     }
+    flush(nlist);
     if (valid) {
         const uint32_t idx = __float_as_uint(me.w);
         sd.accel[idx] = make_float4(acc.fx(), acc.fy(), 0.f, 0.f);
@@ -1185,6 +1353,80 @@ __global__ void k_export_entries(const SimDesc* __restrict__ sims, uint32_t sim,
     }
 }
 
+// ===================================================== direct probes =====
+
+constexpr int kProbeThreads = 256;
+constexpr int kProbesPerBlock = 8;
+
+// FP64 direct sums for probe bodies (direct_acceleration_for,
+// nbody/src/lib.rs:315-329, over the f32 state promoted to f64): every term
+// is nbody/src/lib.rs:247-255 with explicit round-to-nearest f64 operations;
+// each thread sums a strided slice of the sources and the block adds the
+// slices in a fixed order.
+__global__ void __launch_bounds__(kProbeThreads) k_direct_probes(
+    const GpuEvolveState* __restrict__ state, uint32_t n, const uint32_t* __restrict__ probes,
+    uint32_t nprobes, double eps, double g, double* __restrict__ out) {
+    __shared__ double sh[kProbesPerBlock][2][kProbeThreads];
+    double tx[kProbesPerBlock], ty[kProbesPerBlock], ax[kProbesPerBlock], ay[kProbesPerBlock];
+    uint32_t ti[kProbesPerBlock];
+#pragma unroll
+    for (int k = 0; k < kProbesPerBlock; ++k) {
+        const uint32_t q = blockIdx.x * kProbesPerBlock + k;
+        ti[k] = q < nprobes ? probes[q] : kNone;
+        const bool ok = ti[k] < n;
+        tx[k] = ok ? (double)state[ti[k]].position_mass[0] : 0.0;
+        ty[k] = ok ? (double)state[ti[k]].position_mass[1] : 0.0;
+        ax[k] = ay[k] = 0.0;
+    }
+    const double eps2 = __dmul_rn(eps, eps);
+    for (uint32_t j = threadIdx.x; j < n; j += kProbeThreads) {
+        const float4 pm = *reinterpret_cast<const float4*>(state + j);
+        const double x = pm.x, y = pm.y, m = pm.z;
+        const double gm = __dmul_rn(g, m);
+#pragma unroll
+        for (int k = 0; k < kProbesPerBlock; ++k) {
+            if (j == ti[k]) continue;
+            const double dx = __dsub_rn(x, tx[k]);
+            const double dy = __dsub_rn(y, ty[k]);
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), eps2);
+            const double inv_r = __ddiv_rn(1.0, __dsqrt_rn(r2));
+            const double scale = __dmul_rn(__dmul_rn(__dmul_rn(gm, inv_r), inv_r), inv_r);
+            ax[k] = __dadd_rn(ax[k], __dmul_rn(dx, scale));
+            ay[k] = __dadd_rn(ay[k], __dmul_rn(dy, scale));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kProbesPerBlock; ++k) {
+        sh[k][0][threadIdx.x] = ax[k];
+        sh[k][1][threadIdx.x] = ay[k];
+    }
+    __syncthreads();
+    for (int stride = kProbeThreads / 2; stride > 0; stride >>= 1) {
+        if ((int)threadIdx.x < stride)
+#pragma unroll
+            for (int k = 0; k < kProbesPerBlock; ++k) {
+                sh[k][0][threadIdx.x] += sh[k][0][threadIdx.x + stride];
+                sh[k][1][threadIdx.x] += sh[k][1][threadIdx.x + stride];
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x < kProbesPerBlock) {
+        const uint32_t q = blockIdx.x * kProbesPerBlock + threadIdx.x;
+        if (q < nprobes) {
+            out[2 * q] = sh[threadIdx.x][0][0];
+            out[2 * q + 1] = sh[threadIdx.x][1][0];
+        }
+    }
+}
+
+cudaError_t launch_direct_probes(const GpuEvolveState* state, uint32_t n, const uint32_t* probes,
+                                 uint32_t nprobes, double eps, double g, double* out,
+                                 cudaStream_t s) {
+    const uint32_t blocks = (nprobes + kProbesPerBlock - 1) / kProbesPerBlock;
+    k_direct_probes<<<blocks, kProbeThreads, 0, s>>>(state, n, probes, nprobes, eps, g, out);
+    return cudaGetLastError();
+}
+
 // ======================================================= conservation =====
 
 constexpr int kConsThreads = 256;
@@ -1284,21 +1526,23 @@ cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
     k_cells<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
                                                  b.keys_a, b.base, b.cell_r, b.cell_end,
                                                  b.cell_child, b.cell_parent, b.cell_counter,
-                                                 b.err);
+                                                 b.groups, b.err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
     k_aggregate<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.npos,
-                                                     b.base, b.sbody, b.cell_r, b.cell_end,
-                                                     b.cell_child, b.cell_parent, b.cell_counter,
-                                                     b.cell_d);
+                                                     b.base, b.sbody, b.keys_a, b.cell_capacity,
+                                                     b.cell_r, b.cell_end, b.cell_child,
+                                                     b.cell_parent, b.cell_counter, b.cell_d,
+                                                     b.groups);
     return cudaGetLastError();
 }
 
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {
-    k_refresh_mac<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(b.sims, b.simout, sim, b.base,
-                                                                 b.cell_d, b.cell_r);
+    k_refresh_mac<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
+        b.sims, b.simout, sim, b.base, b.keys_a, b.cell_capacity, b.cell_end, b.cell_parent,
+        b.cell_d, b.cell_r, b.groups);
     return cudaGetLastError();
 }
 
@@ -1306,9 +1550,9 @@ cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potent
                             cudaStream_t s) {
     const uint32_t blocks = (b.nchunks + kTravWarps - 1) / kTravWarps;
 #define GBH_TRAVERSE(C, P, S)                                                                   \
-    k_traverse<C, P, S><<<blocks, kTravWarps * 32, 0, s>>>(b.sims, b.simout, b.chunk_sim,      \
-                                                           b.nchunks, b.sbody, b.cell_r,       \
-                                                           b.cell_d, b.base, b.force_stats)
+    k_traverse<C, P, S><<<blocks, kTravWarps * 32, 0, s>>>(                                  \
+        b.sims, b.simout, b.chunk_sim, b.nchunks, b.sbody, b.groups, b.cell_d, b.cell_capacity, \
+        b.force_stats, b.err)
     if (stats) {
         if (compensated) {
             if (potential) GBH_TRAVERSE(true, true, true); else GBH_TRAVERSE(true, false, true);

@@ -366,6 +366,30 @@ class NbodyGpu:
         check(_lib.load().galaxy_bh_state_bytes(evolving.handle, C.byref(v)))
         return int(v.value)
 
+    def direct_probes(self, evolving: EvolvingState, config: Config, probes) -> np.ndarray:
+        """FP64 direct accelerations (k, 2) of the probe bodies on the device
+        (direct_acceleration_for, nbody/src/lib.rs:315-329)."""
+        p = np.ascontiguousarray(probes, dtype=np.uint32)
+        out = np.zeros((len(p), 2))
+        c = config.to_c()
+        check(_lib.load().galaxy_bh_direct_probes(self._h.p, evolving.handle, C.byref(c), ptr(p),
+                                                  len(p), ptr(out)))
+        return out
+
+    def probe_error(self, evolving: EvolvingState, config: Config, probes) -> dict:
+        """Median / p99 / max relative error of the resident accelerations
+        against FP64 direct sums at the probe bodies (probe_error,
+        nbody/src/lib.rs:370-395, with percentiles)."""
+        p = np.ascontiguousarray(probes, dtype=np.uint32)
+        exact = self.direct_probes(evolving, config, p)
+        acc, _ = self.read_evolving_accelerations(evolving)
+        a = acc[p]
+        den = np.maximum(np.hypot(exact[:, 0], exact[:, 1]), 1e-30)
+        rel = np.hypot(a[:, 0] - exact[:, 0], a[:, 1] - exact[:, 1]) / den
+        return {"probes": int(len(p)), "median": float(np.median(rel)),
+                "p99": float(np.quantile(rel, 0.99)), "max": float(rel.max()),
+                "rms": float(np.sqrt(np.mean(rel ** 2)))}
+
     def conservation(self, evolving: EvolvingState) -> dict:
         """FP64 invariants of the resident state (galaxy-bh-evolve.rs:252-278
         plus kinetic, potential and total energy)."""

@@ -210,6 +210,17 @@ int galaxy_bh_force_into(bh_device* dev, bh_state* st, const BhSettings* setting
 int galaxy_bh_step(bh_device* dev, bh_state* st, bh_tree* tree, const bh_config* cfg, double dt,
                    uint32_t nsteps);
 
+/* ---- FP64 direct-sum probes ---------------------------------------------------
+ * direct_acceleration_for (nbody/src/lib.rs:315-329) on the device for
+ * nprobes body indices of the resident state, in f64 with the reference's
+ * per-term arithmetic (only the summation order is parallel).  out receives
+ * ax, ay per probe (2*nprobes doubles, host memory); cfg supplies softening
+ * and G.  The reference runs these probes on the CPU (probe_error,
+ * nbody/src/lib.rs:370-395); the engine uses them to state the FP64 error of
+ * every run. */
+int galaxy_bh_direct_probes(bh_device* dev, bh_state* st, const bh_config* cfg,
+                            const uint32_t* probes, uint32_t nprobes, double* out);
+
 /* ---- FP64 conservation reductions ------------------------------------------
  * Deterministic f64 sums over the resident f32 state: out[0..9] = mass,
  * com_x, com_y, px, py, lz, kinetic energy, potential energy (0 unless the

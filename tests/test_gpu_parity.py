@@ -313,3 +313,42 @@ def test_conservation_f64(gpu):
     assert c["lz"] == pytest.approx(lz, rel=1e-12)
     ke = 0.5 * (m * (b[:, 2] ** 2 + b[:, 3] ** 2)).sum()
     assert c["kinetic"] == pytest.approx(ke, rel=1e-12)
+
+
+def test_fp64_direct_probes_match_oracle(gpu, oracle):
+    """galaxy_bh_direct_probes vs direct_acceleration_for (lib.rs:315-329):
+    identical f64 terms, parallel summation order -> 1e-12 relative."""
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.binary_encounter(30000, 3)
+    ev, _ = gpu.create_evolving_state(bodies)
+    b32 = f32_bodies(bodies)
+    probes = np.random.default_rng(2).choice(len(bodies), 257, replace=False).astype(np.uint32)
+    got = gpu.direct_probes(ev, cfg, probes)
+    want = oracle.direct_accelerations_for(b32, ocfg(oracle, cfg), probes)
+    assert oracle.relative_errors(got, want).max() < 1e-12
+
+
+def test_config1_disc_trajectory_100_steps(gpu, rt, oracle):
+    """Rotating exponential disc, N=16384, eps 0.01, theta 0.5, bucket 1,
+    100 KDK steps at dt 1e-3, seed 42: the GPU f32 trajectory stays within
+    the reference's trajectory gates (galaxy-bh-gpu-tree-parallel.rs:409-412)
+    of the f64 reference CPU path run on the same initial state."""
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.exponential_disc(16384, 42)
+    b32 = f32_bodies(bodies)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    rt.step(gpu, ev, tree, cfg, 1e-3, 100)
+    final, _ = gpu.read_evolving_state(ev)
+    ref = oracle.cpu_flat_evolve(b32, 100, 1e-3, ocfg(oracle, cfg),
+                                 nthreads=oracle.nthreads_default())
+    pd = np.hypot(final[:, 0] - ref[:, 0], final[:, 1] - ref[:, 1])
+    pr = np.hypot(ref[:, 0], ref[:, 1])
+    vd = np.hypot(final[:, 2] - ref[:, 2], final[:, 3] - ref[:, 3])
+    vr = np.hypot(ref[:, 2], ref[:, 3])
+    assert np.sqrt((pd ** 2).sum() / (pr ** 2).sum()) < 0.03
+    assert np.sqrt((vd ** 2).sum() / (vr ** 2).sum()) < 0.03
+    assert (pd / np.maximum(pr, 1e-6)).max() < 0.30
+    assert (vd / np.maximum(vr, 1e-9)).max() < 0.30
