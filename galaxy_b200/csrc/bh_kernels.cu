@@ -555,76 +555,113 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
 
 // =============================================================== cells ====
 
-// End (exclusive, sim-local) of the depth-d group containing sorted position
-// i, searching from `from`.
-__device__ __forceinline__ uint32_t group_end(const uint32_t* __restrict__ sc, uint32_t n,
-                                              uint32_t i, uint32_t d, uint32_t from) {
-    if (d == 0) return n;
-    const uint32_t sh = 32u - 2u * d;
-    const unsigned long long next = ((unsigned long long)(sc[i] >> sh) + 1ull) << sh;
-    if (next > 0xffffffffull) return n;
-    return gallop_lower_bound(sc, from, n, (uint32_t)next);
-}
+// One thread per cell.  A block covers 256 positions, whose cells are the
+// contiguous preorder range [base[P0], base[P0 + 256]); the codes and chain
+// bases of the next kCellsWin positions sit in shared memory, so the range
+// searches of almost every cell (all but the few that span more than the
+// window) never touch global memory.
+constexpr uint32_t kCellsThreads = 256;
+constexpr uint32_t kCellsWin = 1024;
+constexpr uint32_t kMaxChain = kMortonDepth + 1;  // cells per position: depths 0..16
 
-__global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
-                                               const uint32_t* __restrict__ chunk_sim,
-                                               uint32_t npos, uint32_t capacity,
-                                               const uint32_t* __restrict__ codes,
-                                               const uint32_t* __restrict__ base, CellRec* cell_r,
-                                               uint32_t* cell_end, uint4* cell_child,
-                                               uint32_t* cell_parent, uint32_t* cell_counter,
-                                               CellRec* groups, uint32_t* err) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npos) return;
-    const uint32_t s = chunk_sim[p >> 5];
-    if (s == kNone) return;
-    const SimDesc& sd = sims[s];
-    const uint32_t i = p - sd.off;
-    if (i >= sd.n) return;
-    const uint32_t k0 = base[p];
-    const uint32_t c = base[p + 1] - k0;
-    if (c == 0) return;
-    if (k0 + c > capacity) {
-        set_err(err, kErrCapacity);
+struct CellsWindow {
+    const uint32_t* s_code;  // codes of positions [w0, w0 + kCellsWin)
+    const uint32_t* s_base;  // base of positions [w0, w0 + kCellsWin]
+    const uint32_t* codes;
+    const uint32_t* base;
+    uint32_t w0;
+
+    __device__ __forceinline__ uint32_t base_at(uint32_t gp) const {
+        const uint32_t j = gp - w0;
+        return j <= kCellsWin ? s_base[j] : base[gp];
+    }
+    // First position in [lo, hi) whose code is >= x, given codes < x before lo
+    // (w0 <= lo).
+    __device__ __forceinline__ uint32_t lower_bound(uint32_t lo, uint32_t hi, uint32_t x) const {
+        const uint32_t wend = min(hi, w0 + kCellsWin);
+        if (lo < wend) {
+            if (s_code[wend - 1u - w0] >= x)
+                return w0 + gallop_lower_bound(s_code, lo - w0, wend - w0, x);
+            lo = wend;
+        }
+        return lo < hi ? gallop_lower_bound(codes, lo, hi, x) : hi;
+    }
+};
+
+__global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restrict__ sims,
+                                                         const uint32_t* __restrict__ chunk_sim,
+                                                         uint32_t npos, uint32_t capacity,
+                                                         const uint32_t* __restrict__ codes,
+                                                         const uint32_t* __restrict__ base,
+                                                         CellRec* cell_r, uint32_t* cell_end,
+                                                         uint4* cell_child, uint32_t* cell_parent,
+                                                         uint32_t* cell_counter, CellRec* groups,
+                                                         uint32_t* err) {
+    __shared__ uint32_t s_code[kCellsWin];
+    __shared__ uint32_t s_base[kCellsWin + 1];
+    __shared__ uint8_t s_owner[kCellsThreads * kMaxChain];  // cell -> position in block
+    const uint32_t t = threadIdx.x;
+    const uint32_t P0 = blockIdx.x * kCellsThreads;
+    for (uint32_t j = t; j <= kCellsWin; j += kCellsThreads) {
+        const uint32_t gp = P0 + j;
+        if (j < kCellsWin) s_code[j] = gp < npos ? codes[gp] : 0xffffffffu;
+        s_base[j] = gp <= npos ? base[gp] : 0u;
+    }
+    __syncthreads();
+    const uint32_t P1 = min(P0 + kCellsThreads, npos);
+    const uint32_t kb = s_base[0], ke = s_base[P1 - P0];
+    if (ke > capacity || ke - kb > kCellsThreads * kMaxChain) {
+        if (t == 0) set_err(err, kErrCapacity);
         return;
     }
-    const uint32_t* sc = codes + sd.off;
-    const uint32_t n = sd.n;
-    const uint32_t dmin = i == 0 ? 0u : shared_levels(sc[i - 1], sc[i]) + 1u;
-    const uint32_t deepest = dmin + c - 1u;
-    uint32_t ends[kMortonDepth + 1];
-    uint32_t from = i + 1;
-    for (int d = (int)deepest; d >= (int)dmin; --d) {
-        from = group_end(sc, n, i, (uint32_t)d, from);
-        ends[d - dmin] = from;
+    if (P0 + t < P1) {
+        const uint32_t c0 = s_base[t] - kb, c = s_base[t + 1] - s_base[t];
+        for (uint32_t j = 0; j < c; ++j) s_owner[c0 + j] = (uint8_t)t;
     }
+    __syncthreads();
+    const CellsWindow w{s_code, s_base, codes, base, P0};
     const uint4 absent = make_uint4(0u, 0u, 0u, kNone);  // u.z == 0: no child in this slot
-    if (dmin == 0) {
-        cell_parent[k0] = kNone;
-        // the simulation's root group holds the root in slot 0 only
-        CellRec* rg = groups + 4ull * (capacity + s);
-        rg[1].u = absent;
-        rg[2].u = absent;
-        rg[3].u = absent;
-    }
-    for (uint32_t d = dmin; d <= deepest; ++d) {
-        const uint32_t k = k0 + (d - dmin);
-        const uint32_t end = ends[d - dmin];
+    for (uint32_t k = kb + t; k < ke; k += kCellsThreads) {
+        const uint32_t tl = s_owner[k - kb];
+        const uint32_t p = P0 + tl;
+        const uint32_t s = chunk_sim[p >> 5];
+        const SimDesc& sd = sims[s];
+        const uint32_t i = p - sd.off;
+        const uint32_t hi = sd.off + sd.n;
+        const uint32_t ci = s_code[tl];
+        const uint32_t dmin =
+            i == 0 ? 0u : shared_levels(tl ? s_code[tl - 1u] : codes[p - 1u], ci) + 1u;
+        const uint32_t k0 = s_base[tl];
+        const uint32_t deepest = dmin + (s_base[tl + 1] - k0) - 1u;
+        const uint32_t d = dmin + (k - k0);
+        // end of the depth-d group holding p
+        uint32_t end = hi;
+        if (d > 0) {
+            const uint32_t sh = 32u - 2u * d;
+            const unsigned long long next = ((unsigned long long)(ci >> sh) + 1ull) << sh;
+            if (next <= 0xffffffffull) end = w.lower_bound(p + 1u, hi, (uint32_t)next);
+        } else {
+            cell_parent[k] = kNone;
+            // the simulation's root group holds the root in slot 0 only
+            CellRec* rg = groups + 4ull * (capacity + s);
+            rg[1].u = absent;
+            rg[2].u = absent;
+            rg[3].u = absent;
+        }
         // u.x (MAC lower bound or leaf body count) and f are filled by k_aggregate
-        cell_r[k].u = make_uint4(0u, base[sd.off + end], p, d);
-        cell_end[k] = sd.off + end;
+        cell_r[k].u = make_uint4(0u, w.base_at(end), p, d);
+        cell_end[k] = end;
         cell_counter[k] = 0;
         uint4 ch = make_uint4(kNone, kNone, kNone, kNone);
         if (d < deepest) {
             const uint32_t sh = 30u - 2u * d;
-            const uint32_t pre = d == 0 ? 0u : (sc[i] >> (32u - 2u * d));
-            uint32_t lo = i;
+            const uint32_t pre = d == 0 ? 0u : (ci >> (32u - 2u * d));
             uint32_t bounds[5];
-            bounds[0] = i;
+            bounds[0] = p;
+            uint32_t lo = p;
 #pragma unroll
             for (uint32_t q = 1; q < 4; ++q) {
-                const uint32_t x = ((pre << 2) | q) << sh;
-                lo = gallop_lower_bound(sc, lo, end, x);
+                lo = w.lower_bound(lo, end, ((pre << 2) | q) << sh);
                 bounds[q] = lo;
             }
             bounds[4] = end;
@@ -632,7 +669,7 @@ __global__ void __launch_bounds__(256) k_cells(const SimDesc* __restrict__ sims,
 #pragma unroll
             for (uint32_t q = 0; q < 4; ++q) {
                 if (bounds[q] < bounds[q + 1]) {
-                    const uint32_t child = bounds[q] == i ? k + 1u : base[sd.off + bounds[q]];
+                    const uint32_t child = bounds[q] == p ? k + 1u : w.base_at(bounds[q]);
                     chp[q] = child;
                     if (child < capacity)
                         cell_parent[child] = k;
@@ -759,76 +796,152 @@ __device__ __forceinline__ SlotRef slot_ref(uint32_t parent, uint32_t depth, uin
     return r;
 }
 
-// Leaves (the last cell of each chain) sum their bodies in Morton order; the
-// last child to finish a parent sums the children in quadrant order
-// 0..3 — the arithmetic and order of nbody/src/flat.rs:179-215, so the f64
-// mass and centre of mass equal the reference's bit for bit.
-__global__ void __launch_bounds__(256) k_aggregate(const SimDesc* __restrict__ sims,
-                                                   const SimOut* __restrict__ simout,
-                                                   const uint32_t* __restrict__ chunk_sim,
-                                                   uint32_t npos, const uint32_t* __restrict__ base,
-                                                   const float4* __restrict__ sbody,
-                                                   const uint32_t* __restrict__ codes,
-                                                   uint32_t capacity, CellRec* cell_r,
-                                                   const uint32_t* __restrict__ cell_end,
-                                                   const uint4* __restrict__ cell_child,
-                                                   const uint32_t* __restrict__ cell_parent,
-                                                   uint32_t* cell_counter, double4* cell_d,
-                                                   CellRec* groups) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npos) return;
-    const uint32_t s = chunk_sim[p >> 5];
-    if (s == kNone) return;
-    const SimDesc& sd = sims[s];
-    if (p - sd.off >= sd.n) return;
-    const uint32_t k0 = base[p];
-    const uint32_t c = base[p + 1] - k0;
-    if (c == 0) return;
-    const double root_half = simout[s].half;
-    const double theta = sd.theta;
-    const float g = sd.g_f;
-    const uint32_t root_group = capacity + s;
-    uint32_t k = k0 + c - 1u;
-    {
-        const uint32_t start = cell_r[k].u.z, end = cell_end[k];
-        double mass = 0.0, wx = 0.0, wy = 0.0;
+// Acquire-release fetch-add at GPU scope: the writes before it (this
+// thread's cell values) are visible to whichever thread reads the counter's
+// final value, and this thread sees the writes released before the
+// increments it reads.
+__device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(p), "r"(v)
+                 : "memory");
+    return old;
+}
+
+struct AggArgs {
+    const SimDesc* sims;
+    const SimOut* simout;
+    const uint32_t* chunk_sim;
+    const float4* sbody;
+    const uint32_t* codes;
+    uint32_t capacity;
+    CellRec* cell_r;
+    const uint32_t* cell_end;
+    const uint4* cell_child;
+    const uint32_t* cell_parent;
+    uint32_t* cell_counter;
+    double4* cell_d;
+    CellRec* groups;
+};
+
+// Aggregates of cell k (u = its record's (lo, skip, start, depth)): a leaf
+// sums its bodies in Morton order, an internal cell its children in quadrant
+// order 0..3 (nbody/src/flat.rs:179-215).
+__device__ __forceinline__ void aggregate_cell(const AggArgs& a, uint32_t k, uint4 u, bool leaf) {
+    const uint32_t start = u.z, depth = u.w, end = a.cell_end[k];
+    const uint32_t s = a.chunk_sim[start >> 5];
+    const SimDesc& sd = a.sims[s];
+    double mass = 0.0, wx = 0.0, wy = 0.0;
+    if (leaf) {
         for (uint32_t q = start; q < end; ++q) {
-            const float4 b = sbody[q];
+            const float4 b = a.sbody[q];
             const double m = (double)b.z;
             mass = __dadd_rn(mass, m);
             wx = __dadd_rn(wx, __dmul_rn(m, (double)b.x));
             wy = __dadd_rn(wy, __dmul_rn(m, (double)b.y));
         }
-        const uint32_t depth = cell_r[k].u.w;
-        store_cell_values(k, mass, wx, wy, depth, start, end - start, true,
-                          slot_ref(cell_parent[k], depth, codes[start], root_group), root_half,
-                          theta, g, cell_d, cell_r, groups);
-    }
-    while (true) {
-        const uint32_t par = cell_parent[k];
-        if (par == kNone) break;
-        const uint4 ch = cell_child[par];
-        const uint32_t nchild = (ch.x != kNone) + (ch.y != kNone) + (ch.z != kNone) + (ch.w != kNone);
-        __threadfence();
-        const uint32_t old = atomicAdd(&cell_counter[par], 1u);
-        if (old + 1u != nchild) break;
-        __threadfence();
-        double mass = 0.0, wx = 0.0, wy = 0.0;
+    } else {
+        const uint4 ch = a.cell_child[k];
         const uint32_t chv[4] = {ch.x, ch.y, ch.z, ch.w};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             if (chv[q] == kNone) continue;
-            const double2 cxy = __ldcg(reinterpret_cast<const double2*>(cell_d + chv[q]));
-            const double cm = __ldcg(reinterpret_cast<const double*>(cell_d + chv[q]) + 2);
+            const double2 cxy = __ldcg(reinterpret_cast<const double2*>(a.cell_d + chv[q]));
+            const double cm = __ldcg(reinterpret_cast<const double*>(a.cell_d + chv[q]) + 2);
             mass = __dadd_rn(mass, cm);
             wx = __dadd_rn(wx, __dmul_rn(cm, cxy.x));
             wy = __dadd_rn(wy, __dmul_rn(cm, cxy.y));
         }
-        const uint32_t pstart = cell_r[par].u.z, pdepth = cell_r[par].u.w;
-        store_cell_values(par, mass, wx, wy, pdepth, pstart, cell_end[par] - pstart, false,
-                          slot_ref(cell_parent[par], pdepth, codes[pstart], root_group),
-                          root_half, theta, g, cell_d, cell_r, groups);
+    }
+    store_cell_values(k, mass, wx, wy, depth, start, end - start, leaf,
+                      slot_ref(a.cell_parent[k], depth, a.codes[start], a.capacity + s),
+                      a.simout[s].half, sd.theta, sd.g_f, a.cell_d, a.cell_r, a.groups);
+}
+
+// Cell k is done and its parent spans several blocks: count k in at the
+// parent; the thread that completes a parent's last child computes the
+// parent and carries on upwards.
+__device__ void climb(const AggArgs& a, uint32_t k) {
+    while (true) {
+        const uint32_t par = a.cell_parent[k];
+        if (par == kNone) return;
+        const uint4 ch = a.cell_child[par];
+        const uint32_t nchild =
+            (ch.x != kNone) + (ch.y != kNone) + (ch.z != kNone) + (ch.w != kNone);
+        if (atomic_add_acq_rel(a.cell_counter + par, 1u) + 1u != nchild) return;
+        aggregate_cell(a, par, a.cell_r[par].u, false);
         k = par;
+    }
+}
+
+// Bottom-up f64 aggregates.  A block covers the cells of 256 positions
+// [P0, P1), the preorder range [kb, ke).  A cell whose positions lie inside
+// [P0, P1) is local: the block computes every leaf first, then its local
+// internal cells depth by depth, deepest first, with a block barrier between
+// depths, so no local cell needs an atomic.  The other cells span several
+// blocks (ancestors of block boundaries, about 1% of the internal cells);
+// each is computed by the thread that completes its last child, found with
+// one acquire-release counter per cell.  Same arithmetic and order as the
+// reference, so the f64 mass and centre of mass equal its values bit for bit.
+// 64 threads per 256 positions: a depth holds few cells, and small blocks
+// let many blocks hide each other's per-depth latency.
+constexpr uint32_t kAggPositions = 256;
+constexpr uint32_t kAggThreads = 64;
+
+__global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint32_t npos,
+                                                           const uint32_t* __restrict__ base,
+                                                           uint32_t* err) {
+    // local internal cells by depth (offsets from kb): one cell per position
+    // and depth, internal depths 0..15
+    __shared__ uint16_t s_level[kMortonDepth][kAggPositions];
+    __shared__ uint32_t s_count[kMortonDepth];
+    __shared__ uint32_t s_code[kAggPositions + 2];  // codes of positions P0-1 .. P0+256
+    const uint32_t t = threadIdx.x;
+    const uint32_t P0 = blockIdx.x * kAggPositions;
+    const uint32_t P1 = min(P0 + kAggPositions, npos);
+    if (t < kMortonDepth) s_count[t] = 0;
+    for (uint32_t j = t; j < kAggPositions + 2; j += kAggThreads) {
+        const uint32_t gp = P0 + j - 1u;
+        s_code[j] = (j > 0 || P0 > 0) && gp < npos ? a.codes[gp] : 0u;
+    }
+    __syncthreads();
+    const uint32_t kb = base[P0], ke = base[P1];
+    // whether the depth-dd group holding position p lies inside [P0, P1):
+    // its neighbours outside the block (within the simulation) differ in
+    // the first dd levels
+    auto inside = [&](uint32_t p, uint32_t dd, const SimDesc& sd) {
+        const uint32_t c = s_code[p - P0 + 1u];
+        const bool left = sd.off >= P0 || shared_levels(s_code[0], c) < dd;
+        const bool right = sd.off + sd.n <= P1 || shared_levels(c, s_code[P1 - P0 + 1u]) < dd;
+        return left && right;
+    };
+    for (uint32_t k = kb + t; k < ke; k += kAggThreads) {
+        const uint4 u = a.cell_r[k].u;  // (0, skip, start, depth)
+        const SimDesc& sd = a.sims[a.chunk_sim[u.z >> 5]];
+        if (u.y == k + 1u) {
+            aggregate_cell(a, k, u, true);
+            if (u.w > 0 && !inside(u.z, u.w - 1u, sd)) climb(a, k);
+        } else if (inside(u.z, u.w, sd)) {
+            if (u.w < kMortonDepth) {
+                const uint32_t slot = atomicAdd(&s_count[u.w], 1u);
+                s_level[u.w][slot] = (uint16_t)(k - kb);
+            } else {
+                set_err(err, kErrCapacity);
+            }
+        }
+    }
+    __syncthreads();
+    for (int d = (int)kMortonDepth - 1; d >= 0; --d) {
+        const uint32_t cnt = s_count[d];
+        if (cnt == 0) continue;
+        for (uint32_t j = t; j < cnt; j += kAggThreads) {
+            const uint32_t k = kb + s_level[d][j];
+            const uint4 u = a.cell_r[k].u;
+            aggregate_cell(a, k, u, false);
+            if (d > 0 && !inside(u.z, (uint32_t)d - 1u, a.sims[a.chunk_sim[u.z >> 5]])) climb(a, k);
+        }
+        __syncthreads();
     }
 }
 
@@ -1523,7 +1636,7 @@ cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
 }
 
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
-    k_cells<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
+    k_cells<<<(b.npos + kCellsThreads - 1) / kCellsThreads, kCellsThreads, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
                                                  b.keys_a, b.base, b.cell_r, b.cell_end,
                                                  b.cell_child, b.cell_parent, b.cell_counter,
                                                  b.groups, b.err);
@@ -1531,11 +1644,11 @@ cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
-    k_aggregate<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, b.simout, b.chunk_sim, b.npos,
-                                                     b.base, b.sbody, b.keys_a, b.cell_capacity,
-                                                     b.cell_r, b.cell_end, b.cell_child,
-                                                     b.cell_parent, b.cell_counter, b.cell_d,
-                                                     b.groups);
+    const AggArgs a{b.sims,          b.simout, b.chunk_sim, b.sbody,      b.keys_a,
+                    b.cell_capacity, b.cell_r, b.cell_end,  b.cell_child, b.cell_parent,
+                    b.cell_counter,  b.cell_d, b.groups};
+    k_aggregate<<<(b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0, s>>>(
+        a, b.npos, b.base, b.err);
     return cudaGetLastError();
 }
 
