@@ -219,6 +219,8 @@ struct bh_state {
     uint32_t* d_chunk_sim = nullptr;
     uint32_t* d_minmax = nullptr;
     double* d_cons = nullptr;  // conservation partials + result
+    uint32_t* d_check = nullptr;         // first invalid record index of the last check
+    GpuEvolveState* d_stage = nullptr;   // upload staging (first galaxy_bh_write_state)
     uint32_t nchunks = 0;
     SimDesc h_sim{};
 };
@@ -257,7 +259,7 @@ extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host
         (e = cudaMalloc(&st->d_accel, sizeof(float4) * (size_t)n)) ||
         (e = cudaMalloc(&st->d_sim, sizeof(SimDesc))) ||
         (e = cudaMalloc(&st->d_chunk_sim, sizeof(uint32_t) * st->nchunks)) ||
-        (e = cudaMalloc(&st->d_minmax, 16))) {
+        (e = cudaMalloc(&st->d_minmax, 16)) || (e = cudaMalloc(&st->d_check, 16))) {
         galaxy_bh_state_destroy(st);
         return cuda_fail(e, "evolving state allocation");
     }
@@ -302,6 +304,8 @@ extern "C" int galaxy_bh_state_destroy(bh_state* st) {
     cudaFree(st->d_chunk_sim);
     cudaFree(st->d_minmax);
     cudaFree(st->d_cons);
+    cudaFree(st->d_check);
+    cudaFree(st->d_stage);
     bh_device* dev = st->dev;
     delete st;
     device_unref(dev);
@@ -373,31 +377,45 @@ extern "C" int galaxy_bh_final_kick(bh_device* dev, bh_state* st, double dt,
     return integrate_state(dev, st, dt, 2, timing);
 }
 
+// Enqueues the record check of n records at `records` (kind 0: evolving
+// states, 1: accelerations) and the copy of its result word to *first_bad.
+static int enqueue_check(bh_state* st, const void* records, int kind, uint32_t n) {
+    bh_device* dev = st->dev;
+    CK(cudaMemsetAsync(st->d_check, 0xff, 4, dev->stream), "memset");
+    CK(launch_check_records(records, kind, n, st->d_check, dev->stream), "record check");
+    return BH_OK;
+}
+
+static int fetch_check(bh_state* st, uint32_t* first_bad) {
+    CK(cudaMemcpyAsync(first_bad, st->d_check, 4, cudaMemcpyDeviceToHost, st->dev->stream),
+       "record check readback");
+    CK(cudaStreamSynchronize(st->dev->stream), "record check readback");
+    return BH_OK;
+}
+
 extern "C" int galaxy_bh_read_state(bh_device* dev, bh_state* st, GpuEvolveState* out,
                                     uint32_t n, bh_stage_timing* timing) {
     int rc = enter(dev);
     if (rc) return rc;
     if (!st || !out) return set_error(BH_INVALID_ARG, "null argument");
     if (n != st->n) return set_error(BH_INVALID_ARG, "readback count %u != resident bodies %u", n, st->n);
+    // nbody_gpu.rs:1043-1053 checks the host copy; the same test runs on the
+    // device records (bitwise the same values) while they are copied out
+    if ((rc = enqueue_check(st, st->d_state, 0, n))) return rc;
     CK(cudaEventRecord(dev->ev[0], dev->stream), "event record");
     CK(cudaMemcpyAsync(out, st->d_state, sizeof(GpuEvolveState) * (size_t)n,
                        cudaMemcpyDeviceToHost, dev->stream),
        "state readback");
     CK(cudaEventRecord(dev->ev[1], dev->stream), "event record");
-    CK(cudaStreamSynchronize(dev->stream), "state readback");
+    uint32_t bad = kNone;
+    if ((rc = fetch_check(st, &bad))) return rc;
     if (timing) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, dev->ev[0], dev->ev[1]);
         *timing = bh_stage_timing{0.0, 0.0, ms * 1e-3};
     }
-    // nbody_gpu.rs:1043-1053
-    for (uint32_t i = 0; i < n; ++i) {
-        const GpuEvolveState& s = out[i];
-        if (!std::isfinite(s.position_mass[0]) || !std::isfinite(s.position_mass[1]) ||
-            !std::isfinite(s.velocity[0]) || !std::isfinite(s.velocity[1]) ||
-            !std::isfinite(s.position_mass[2]) || !(s.position_mass[2] > 0.f))
-            return set_error(BH_NONFINITE, "GPU produced invalid evolving body state at %u", i);
-    }
+    if (bad != kNone)
+        return set_error(BH_NONFINITE, "GPU produced invalid evolving body state at %u", bad);
     return BH_OK;
 }
 
@@ -407,21 +425,22 @@ extern "C" int galaxy_bh_read_accel(bh_device* dev, bh_state* st, GpuAccel* out,
     if (rc) return rc;
     if (!st || !out) return set_error(BH_INVALID_ARG, "null argument");
     if (n != st->n) return set_error(BH_INVALID_ARG, "readback count %u != resident bodies %u", n, st->n);
+    // nbody_gpu.rs:1097-1101, evaluated on the device records
+    if ((rc = enqueue_check(st, st->d_accel, 1, n))) return rc;
     CK(cudaEventRecord(dev->ev[0], dev->stream), "event record");
     CK(cudaMemcpyAsync(out, st->d_accel, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost,
                        dev->stream),
        "acceleration readback");
     CK(cudaEventRecord(dev->ev[1], dev->stream), "event record");
-    CK(cudaStreamSynchronize(dev->stream), "acceleration readback");
+    uint32_t bad = kNone;
+    if ((rc = fetch_check(st, &bad))) return rc;
     if (timing) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, dev->ev[0], dev->ev[1]);
         *timing = bh_stage_timing{0.0, 0.0, ms * 1e-3};
     }
-    // nbody_gpu.rs:1097-1101
-    for (uint32_t i = 0; i < n; ++i)
-        if (!std::isfinite(out[i].value[0]) || !std::isfinite(out[i].value[1]))
-            return set_error(BH_NONFINITE, "GPU produced invalid evolving acceleration at %u", i);
+    if (bad != kNone)
+        return set_error(BH_NONFINITE, "GPU produced invalid evolving acceleration at %u", bad);
     return BH_OK;
 }
 
@@ -431,11 +450,20 @@ extern "C" int galaxy_bh_write_state(bh_device* dev, bh_state* st, const GpuEvol
     if (rc) return rc;
     if (!st || !host) return set_error(BH_INVALID_ARG, "null argument");
     if (n != st->n) return set_error(BH_INVALID_ARG, "write count %u != resident bodies %u", n, st->n);
-    if ((rc = check_state_records(host, n))) return rc;
-    CK(cudaMemcpyAsync(st->d_state, host, sizeof(GpuEvolveState) * (size_t)n,
+    // Upload into a staging buffer, check the records there and only then
+    // replace the resident state: an invalid upload leaves it untouched.
+    if (!st->d_stage)
+        CK(cudaMalloc(&st->d_stage, sizeof(GpuEvolveState) * (size_t)n), "staging allocation");
+    CK(cudaMemcpyAsync(st->d_stage, host, sizeof(GpuEvolveState) * (size_t)n,
                        cudaMemcpyHostToDevice, dev->stream),
        "state upload");
-    CK(cudaStreamSynchronize(dev->stream), "state upload");
+    if ((rc = enqueue_check(st, st->d_stage, 0, n))) return rc;
+    uint32_t bad = kNone;
+    if ((rc = fetch_check(st, &bad))) return rc;
+    if (bad != kNone) return set_error(BH_NONFINITE, "body %u contains invalid evolving state", bad);
+    CK(cudaMemcpyAsync(st->d_state, st->d_stage, sizeof(GpuEvolveState) * (size_t)n,
+                       cudaMemcpyDeviceToDevice, dev->stream),
+       "state upload");
     return BH_OK;
 }
 

@@ -139,6 +139,11 @@ cudaError_t launch_conservation(const GpuEvolveState* state, const float* potent
                                 double* partials, uint32_t nblocks, double* out,
                                 cudaStream_t s);
 uint32_t conservation_blocks(uint32_t n);
+// Record validity check: *first_bad (preset to all ones) gets the smallest
+// index of a record that fails it.  kind 0: evolving states (finite position,
+// velocity and mass, mass > 0); kind 1: accelerations (finite x, y).
+cudaError_t launch_check_records(const void* records, int kind, uint32_t n, uint32_t* first_bad,
+                                 cudaStream_t s);
 
 // Sets the calling thread's last-error message (bh_engine.cu); returns status.
 int set_error_message(int status, const char* message);

@@ -1718,4 +1718,40 @@ cudaError_t launch_conservation(const GpuEvolveState* state, const float* potent
     return cudaGetLastError();
 }
 
+
+// ============================================================ checks ====
+
+// The readback checks of nbody_gpu.rs:1043-1053 (states) and 1097-1101
+// (accelerations), evaluated on the device copy of the records.
+template <int KIND>
+__global__ void __launch_bounds__(256) k_check_records(const float4* __restrict__ rec, uint32_t n,
+                                                       uint32_t* first_bad) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        bool ok;
+        if (KIND == 0) {
+            const float4 pm = rec[2ull * i];
+            const float4 v = rec[2ull * i + 1];
+            ok = isfinite(pm.x) && isfinite(pm.y) && isfinite(v.x) && isfinite(v.y) &&
+                 isfinite(pm.z) && pm.z > 0.f;
+        } else {
+            const float4 a = rec[i];
+            ok = isfinite(a.x) && isfinite(a.y);
+        }
+        if (!ok) atomicMin(first_bad, i);
+    }
+}
+
+cudaError_t launch_check_records(const void* records, int kind, uint32_t n, uint32_t* first_bad,
+                                 cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t want = (n + 255ull) / 256ull;
+    const uint32_t blocks = (uint32_t)(want < 148ull * 16ull ? want : 148ull * 16ull);
+    if (kind == 0)
+        k_check_records<0><<<blocks, 256, 0, s>>>(static_cast<const float4*>(records), n, first_bad);
+    else
+        k_check_records<1><<<blocks, 256, 0, s>>>(static_cast<const float4*>(records), n, first_bad);
+    return cudaGetLastError();
+}
+
 }  // namespace gbh

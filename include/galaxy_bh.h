@@ -152,13 +152,19 @@ int galaxy_bh_state_bytes(bh_state* st, uint64_t* bytes);
 int galaxy_bh_kick_drift(bh_device* dev, bh_state* st, double dt, bh_stage_timing* timing);
 int galaxy_bh_final_kick(bh_device* dev, bh_state* st, double dt, bh_stage_timing* timing);
 /* NbodyGpu::read_evolving_state (nbody_gpu.rs:1019-1069); fails with
- * BH_NONFINITE on non-finite values or mass <= 0 like the reference. */
+ * BH_NONFINITE on non-finite values or mass <= 0 like the reference, naming
+ * the first such record (checked on the device while the copy runs; `out`
+ * still receives every record). */
 int galaxy_bh_read_state(bh_device* dev, bh_state* st, GpuEvolveState* out, uint32_t n,
                          bh_stage_timing* timing);
 /* NbodyGpu::read_evolving_accelerations (nbody_gpu.rs:1071-1114). */
 int galaxy_bh_read_accel(bh_device* dev, bh_state* st, GpuAccel* out, uint32_t n,
                          bh_stage_timing* timing);
-/* Overwrites the resident state in place (checkpoint resume). */
+/* Overwrites the resident state (checkpoint resume).  The records are
+ * uploaded to a staging buffer (allocated by the first call) and checked
+ * there like galaxy_bh_state_create's input; an invalid record fails the
+ * call with BH_NONFINITE, naming the first one, and leaves the resident
+ * state unchanged. */
 int galaxy_bh_write_state(bh_device* dev, bh_state* st, const GpuEvolveState* host, uint32_t n);
 
 /* ---- GPU-built tree ------------------------------------------------------

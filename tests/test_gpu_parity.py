@@ -352,3 +352,48 @@ def test_config1_disc_trajectory_100_steps(gpu, rt, oracle):
     assert np.sqrt((vd ** 2).sum() / (vr ** 2).sum()) < 0.03
     assert (pd / np.maximum(pr, 1e-6)).max() < 0.30
     assert (vd / np.maximum(vr, 1e-9)).max() < 0.30
+
+
+def test_state_upload_and_readback_checks(gpu, oracle):
+    """write_state rejects an invalid record (reporting the first bad index)
+    and leaves the resident state as it was; read_state reports the first
+    record whose values are no longer finite (nbody_gpu.rs:1043-1053)."""
+    from galaxy_b200 import _lib
+    import ctypes as C
+    bodies = scenarios.exponential_disc(3000, 5)
+    ev, _ = gpu.create_evolving_state(bodies)
+    s0, _ = gpu.read_evolving_state_records(ev)
+    L = _lib.load()
+    bad = s0.copy()
+    recs = bad.view(np.float32).reshape(-1, 8)
+    recs[1234, 2] = 0.0     # mass 0
+    recs[2500, 4] = np.nan  # later, non-finite velocity
+    rc = L.galaxy_bh_write_state(gpu.handle, ev.handle, _lib.ptr(bad), len(bad))
+    assert rc == _lib.BH_NONFINITE
+    assert "1234" in _lib.last_error()
+    got, _ = gpu.read_evolving_state_records(ev)
+    assert np.array_equal(got.view(np.uint32), s0.view(np.uint32))
+    # a valid upload replaces the state bit for bit
+    s1 = s0.copy()
+    r1 = s1.view(np.float32).reshape(-1, 8)
+    r1[:, 0] += np.float32(0.25)
+    r1[777, 4] = 1e30    # finite, but its drift below overflows f32
+    r1[1500, 5] = -2e30
+    _lib.check(L.galaxy_bh_write_state(gpu.handle, ev.handle, _lib.ptr(s1), len(s1)))
+    got, _ = gpu.read_evolving_state_records(ev)
+    assert np.array_equal(got.view(np.uint32), s1.view(np.uint32))
+    # a drift that overflows f32 positions fails the readback at the first
+    # overflowing record, as the f32 restatement of the kick predicts
+    dt = 1.0e10
+    a32, _ = gpu.read_evolving_accelerations_f32(ev)
+    want = oracle.f32_kick_drift(s1.view(np.float32).reshape(-1, 8), a32, dt)
+    ok = (np.isfinite(want[:, [0, 1, 4, 5, 2]]).all(axis=1)) & (want[:, 2] > 0)
+    assert not ok.all()
+    first = int(np.argmin(ok))
+    assert first == 777
+    gpu.kick_drift(ev, dt)
+    out = np.zeros(len(s1), _lib.EVOLVE_STATE_DTYPE)
+    rc = L.galaxy_bh_read_state(gpu.handle, ev.handle, _lib.ptr(out), len(out), None)
+    assert rc == _lib.BH_NONFINITE
+    assert f"at {first}" in _lib.last_error()
+    assert np.array_equal(out.view(np.float32).reshape(-1, 8), want)
