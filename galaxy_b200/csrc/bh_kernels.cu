@@ -1067,6 +1067,7 @@ __global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_tr
     unsigned long long* stats, uint32_t* err) {
     __shared__ uint2 s_stack[kTravWarps][kTravStack];  // (node group, lane mask)
     __shared__ float4 s_list[kTravWarps][kTravList];   // (com_x, com_y, G*m, lane mask bits)
+    __shared__ uint4 s_mix[kTravWarps][32];  // mixed slots: (group, slot, lane mask, opened)
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t chunk = blockIdx.x * kTravWarps + warp;
@@ -1105,12 +1106,17 @@ __global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_tr
         acc.add(dx * scale, dy * scale);
         if (POT) phi -= take ? gm * inv_r : 0.f;
     };
+    const uint32_t lane_bit = 1u << lane;
     auto flush = [&](uint32_t count) {
 #pragma unroll 4
         for (uint32_t i = 0; i < count; ++i) {
             const float4 e = list[i];
             const float dx = e.x - tx, dy = e.y - ty;
-            term(dx, dy, dist2(dx, dy), e.z, (__float_as_uint(e.w) >> lane) & 1u);
+            const float inv_r = rsqrtf(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, eps2)));
+            const float gm = (__float_as_uint(e.w) & lane_bit) ? e.z : 0.f;
+            const float scale = gm * inv_r * inv_r * inv_r;
+            acc.add(dx * scale, dy * scale);
+            if (POT) phi -= gm * inv_r;
         }
     };
 
@@ -1172,43 +1178,43 @@ __global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_tr
         }
         if (STATS) ++n_iter;
 
-        // mixed cells: every lane of the mask decides for itself
-        uint32_t bm = __ballot_sync(kFull, mixed);
-        while (bm) {
-            const uint32_t src = __ffs(bm) - 1u;
-            bm &= bm - 1u;
-            const float cx = __shfl_sync(kFull, f.x, src);
-            const float cy = __shfl_sync(kFull, f.y, src);
-            const float gm = __shfl_sync(kFull, f.z, src);
-            const float hi = __shfl_sync(kFull, f.w, src);
-            const float lo = __uint_as_float(__shfl_sync(kFull, u.x, src));
-            const uint32_t start = __shfl_sync(kFull, u.y, src);
-            const uint32_t count = __shfl_sync(kFull, u.z, src);
-            const uint32_t k = __shfl_sync(kFull, u.w, src);
-            const uint32_t M = __shfl_sync(kFull, A, src);
-            const bool active = (M >> lane) & 1u;
-            const bool holds = (p - start) < count;
-            const float dx = cx - tx, dy = cy - ty;
+        // mixed cells: every lane of the mask decides for itself, one cell
+        // after the other (records re-read through L1, masks through shared)
+        const uint32_t bm = __ballot_sync(kFull, mixed);
+        const uint32_t mrank = __popc(bm & lanes_below);
+        if (mixed) s_mix[warp][mrank] = make_uint4(e.x, lane & 3u, A, 0u);
+        __syncwarp();
+        const uint32_t nm = __popc(bm);
+        for (uint32_t i = 0; i < nm; ++i) {
+            const uint4 mx = s_mix[warp][i];
+            const CellRec* r = groups + 4ull * mx.x + mx.y;
+            const float4 cf = __ldg(&r->f);
+            const uint4 cu = __ldg(&r->u);
+            const bool active = (mx.z & lane_bit) != 0u;
+            const bool holds = (p - cu.y) < cu.z;
+            const float dx = cf.x - tx, dy = cf.y - ty;
             const float d2 = dist2(dx, dy);
-            bool approx = active && !holds && d2 > hi;
-            bool open = active && (holds || d2 < lo);
+            bool approx = active && !holds && d2 > cf.w;
+            bool open = active && (holds || d2 < __uint_as_float(cu.x));
             const bool undecided = active && !approx && !open;
             if (__any_sync(kFull, undecided)) {
                 if (undecided) {
-                    approx = exact_mac(cell_d, k, tx, ty, simout[s].half,
-                                       __float_as_uint(hi) & 31u, sd.theta);
+                    approx = exact_mac(cell_d, cu.w, tx, ty, simout[s].half,
+                                       __float_as_uint(cf.w) & 31u, sd.theta);
                     open = !approx;
                     if (STATS) ++n_exact;
                 }
             }
             if (__any_sync(kFull, approx)) {
-                term(dx, dy, d2, gm, approx);
+                term(dx, dy, d2, cf.z, approx);
                 if (STATS) n_approx += approx;
             }
             const uint32_t O = __ballot_sync(kFull, open);
-            if (lane == src) op = O;
+            if (lane == 0) s_mix[warp][i].w = O;
             if (STATS) ++n_iter;
         }
+        __syncwarp();
+        if (mixed) op = s_mix[warp][mrank].w;
 
         // leaves of several bodies: each body summed directly, self excluded
         uint32_t bl = __ballot_sync(kFull, multi);
