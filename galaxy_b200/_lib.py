@@ -30,6 +30,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CAPACITY_OVERFLOW", 3: "NONFINITE
 
 BH_FLAG_COMPENSATED = 1
 BH_FLAG_POTENTIAL = 2
+BH_FLAG_NO_STATS = 4
 
 # Frozen record dtypes (runtime/src/nbody_gpu.rs:22-83), all little-endian.
 EVOLVE_STATE_DTYPE = np.dtype([("position_mass", "<f4", (4,)), ("velocity", "<f4", (4,))])

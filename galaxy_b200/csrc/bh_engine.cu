@@ -992,9 +992,10 @@ extern "C" int galaxy_bh_force(bh_device* dev, bh_state* st, bh_tree* tree, cons
         b->built_g = cfg->g;
     }
     CK(cudaEventRecord(dev->ev[0], dev->stream), "event");
-    if ((rc = enqueue_force(tree->batch, true))) return rc;
+    const bool stats = !(cfg->flags & BH_FLAG_NO_STATS);
+    if ((rc = enqueue_force(tree->batch, stats))) return rc;
     if ((rc = stage_time(dev, timing))) return rc;
-    tree->batch->stats_valid = true;
+    tree->batch->stats_valid = stats;
     return check_device_errors(tree->batch);
 }
 

@@ -18,8 +18,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (BH_FLAG_COMPENSATED, BH_FLAG_POTENTIAL, BhBuildTiming, BhConfig,
-                   BhForceStats, BhStageTiming, EngineError, EngineUnavailable, check, ptr)
+from ._lib import (BH_FLAG_COMPENSATED, BH_FLAG_NO_STATS, BH_FLAG_POTENTIAL, BhBuildTiming,
+                   BhConfig, BhForceStats, BhStageTiming, EngineError, EngineUnavailable, check,
+                   ptr)
 
 G_KPC3_PER_MSUN_MYR2 = 4.498502151575286e-12  # nbody/src/lib.rs:6
 DEFAULT_THETA = 0.5
@@ -46,6 +47,7 @@ class Config:
     max_depth: int = DEFAULT_MAX_DEPTH
     compensated: bool = False
     potential: bool = False
+    force_stats: bool = True  # ParallelTreeRuntime.force also counts visits/terms
 
     def validate(self) -> None:
         if not np.isfinite(self.theta) or self.theta < 0.0:
@@ -62,7 +64,8 @@ class Config:
     def to_c(self) -> BhConfig:
         self.validate()
         flags = (BH_FLAG_COMPENSATED if self.compensated else 0) | (
-            BH_FLAG_POTENTIAL if self.potential else 0)
+            BH_FLAG_POTENTIAL if self.potential else 0) | (
+            0 if self.force_stats else BH_FLAG_NO_STATS)
         return BhConfig(float(self.theta), float(self.softening_kpc), float(self.g),
                         int(self.bucket), int(self.max_depth), flags, 0)
 

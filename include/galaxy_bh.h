@@ -88,6 +88,7 @@ typedef struct {
 
 #define BH_FLAG_COMPENSATED 1u /* two-sum compensated force accumulation */
 #define BH_FLAG_POTENTIAL   2u /* also accumulate the softened potential */
+#define BH_FLAG_NO_STATS    4u /* galaxy_bh_force skips its force statistics */
 
 /* StageTiming of nbody_gpu.rs:125-130 (seconds). */
 typedef struct {
