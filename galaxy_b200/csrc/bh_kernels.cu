@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
 
 // ============================================================== radix =====
 
+constexpr int kLookWindow = 8;  // predecessor flags loaded per look-back round trip
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = (1u << 30) - 1u;
@@ -395,21 +396,36 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     atomicExch(my_flag, (first ? kFlagInc : kFlagAgg) | run);
     uint32_t excl = 0;
     if (!first) {
+        // look back kLookWindow predecessors per round trip: add aggregates
+        // up to the nearest inclusive prefix; re-poll from the first tile
+        // that has not published yet.  The simulation's first tile is
+        // inclusive, so the window never needs tiles before it.
         uint32_t tp = t - 1;
         const long long t0 = clock64();
         while (true) {
-            const uint32_t f = ld_volatile(flags + (size_t)tp * kRadixDigits + d);
-            const uint32_t st = f & ~kFlagMask;
-            if (st == 0u) {
-                if (clock64() - t0 > kSpinCycles) {
-                    set_err(err, kErrLookbackTimeout);
-                    break;
-                }
-                continue;
+            uint32_t f[kLookWindow];
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j)
+                f[j] = tp >= sd.first_tile + j
+                           ? ld_volatile(flags + (size_t)(tp - j) * kRadixDigits + d)
+                           : 0u;
+            bool done = false;
+            int used = 0;
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j) {
+                if (done || used < j) continue;
+                const uint32_t st = f[j] & ~kFlagMask;
+                if (st == 0u) continue;
+                excl += f[j] & kFlagMask;
+                used = j + 1;
+                done = st == kFlagInc;
             }
-            excl += f & kFlagMask;
-            if (st == kFlagInc) break;
-            --tp;
+            if (done) break;
+            tp -= used;
+            if (used < kLookWindow && clock64() - t0 > kSpinCycles) {
+                set_err(err, kErrLookbackTimeout);
+                break;
+            }
         }
         atomicExch(my_flag, kFlagInc | (excl + run));
     }
@@ -526,18 +542,27 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
             uint32_t tp = t - 1;
             const long long c0 = clock64();
             while (true) {
-                const unsigned long long f = ld_volatile64(&flags[tp]);
-                const unsigned long long st = f & ~kScanMask;
-                if (st == 0ull) {
-                    if (clock64() - c0 > kSpinCycles) {
-                        set_err(err, kErrLookbackTimeout);
-                        break;
-                    }
-                    continue;
+                unsigned long long f[kLookWindow];
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j)
+                    f[j] = tp >= (uint32_t)j ? ld_volatile64(&flags[tp - j]) : 0ull;
+                bool done = false;
+                int used = 0;
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j) {
+                    if (done || used < j) continue;
+                    const unsigned long long st = f[j] & ~kScanMask;
+                    if (st == 0ull) continue;
+                    excl += f[j] & kScanMask;
+                    used = j + 1;
+                    done = st == kScanInc;
                 }
-                excl += f & kScanMask;
-                if (st == kScanInc) break;
-                --tp;
+                if (done) break;
+                tp -= used;
+                if (used < kLookWindow && clock64() - c0 > kSpinCycles) {
+                    set_err(err, kErrLookbackTimeout);
+                    break;
+                }
             }
             atomicExch(&flags[t], kScanInc | (excl + tile_total));
         }
