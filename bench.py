@@ -35,25 +35,27 @@ sys.path.insert(0, ROOT)
 N_BODIES = 1 << 20
 THETA, EPS, G, BUCKET, DT, SEED = 0.5, 0.005, 1.0, 1, 5e-4, 7
 METRIC = "particle-steps/s"
+# ncu DRAM bytes (read + write) of integrate, Morton, 4 radix passes, count/scan,
+# cells and aggregate for one step at N=2^20 (profiles/build_dram_N2p20.md)
+BUILD_DRAM_BYTES_PER_STEP = 687.0e6
 WORKLOAD = "cold-collapse uniform disc N=2^20, eps=0.005, theta=0.5, bucket=1, dt=5e-4, seed 7"
 
 def algorithmic_bytes(c: float) -> dict:
-    """Bytes each HBM-bound stage must move per body (reads + writes),
-    counted from the records it touches; c = cells per body (measured)."""
+    """Bytes per body-step each HBM-bound stage must move (reads + writes) in
+    the reference's record layout (32 B state, 16 B accel, 8 B key+index,
+    64 B cells); c = cells per body (measured).  Total 264 + 160c."""
     return {
-        # kick/drift: read 32 B state + 16 B accel, write 32 B state
+        # fused leapfrog + bounds partials: read 32 B state + 16 B accel, write 32 B
         "integrate": 80.0,
-        # Morton: read x,y (8 B), write 4 B code
-        "morton": 12.0,
-        # radix: pass 0 reads 4 B key, writes 8 B; passes 1-3 read 8 B write 8 B;
-        # last pass gathers 16 B of state and writes a 16 B sorted body
-        "radix": 4 + 8 + 3 * 16 + 16 + 16,
-        # count+scan reads codes (4 B) writes base (4 B); cells read codes/base
-        # and write 16 B range + 16 B children + 4 B parent + 4 B counter per cell
-        "topology": 8 + 8 + c * 40.0,
-        # aggregate: sorted bodies 16 B + base 8 B; per cell read 16 B range +
-        # 16 B children + 4 B parent + 4 B counter, write 32 B f64 + 16 B f32
-        "aggregate": 24 + c * 88.0,
+        # Morton: read 32 B state, write 8 B key+index
+        "morton": 40.0,
+        # 4 stable 8-bit passes (4 + 4x16) plus positions and the sorted
+        # gather (read 4 + 32, write 4 + 16), which the last pass performs
+        "radix": 68.0 + 56.0,
+        # topology: read 4 B codes, write 64 B per cell
+        "topology": 4.0 + 64.0 * c,
+        # aggregates: read 64 B per cell + 16 B sorted body, write 32 B per cell
+        "aggregate": 16.0 + 96.0 * c,
     }
 
 
@@ -362,6 +364,9 @@ def run_engine(args, world, rank, local, pg):
     if not args.no_served:
         served = run_served_leg(gpu, capacity=(batched or {}).get("value", value / world)
                                 / max(world, 1))
+    precision = None
+    if not args.no_precision:
+        precision = run_precision_leg(gpu, steps=args.precision_steps)
     if rank != 0:
         if pg:
             pg.barrier()
@@ -378,7 +383,10 @@ def run_engine(args, world, rank, local, pg):
                    "l2": "working set > L2 (state 32 MiB + accel 16 MiB + sort 24 MiB + "
                          f"cells {evid_meta_cells * 104 / 2**20:.0f} MiB per step)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     # dram__bytes_read.sum + dram__bytes_write.sum of the build and
+                     # leapfrog kernels of one step (profiles/build_dram_N2p20.md)
+                     "traffic": BUILD_DRAM_BYTES_PER_STEP,
                      "kernels": "sort/build/leapfrog (integrate+bounds, morton, 4 radix "
                                 "passes, count/scan, cells, aggregate)",
                      "peak_source": peaks["source"],
@@ -405,6 +413,7 @@ def run_engine(args, world, rank, local, pg):
         "at_1e-3_force_error": accurate,
         "batched": batched,
         "served": served,
+        "precision": precision,
         "clocks": clk,
         "gpu_launches": 10 * args.steps + 1,
         "gpu": gpu.info().get("name"),
@@ -413,6 +422,76 @@ def run_engine(args, world, rank, local, pg):
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def run_precision_leg(gpu, steps: int = 500, n: int = 1 << 22, every: int = 10,
+                      probes: int = 8192, thetas=(0.3, 0.5, 0.7)) -> dict:
+    """Precision form: a binary disc encounter of two 2^21-body exponential
+    discs (scale lengths 1.0 / 0.7, masses 1 : 0.5, 8 apart, relative speed
+    0.3), f32 state with compensated two-sum force sums, eps 0.005, dt 5e-4.
+    Per theta: FP64 energy / momentum / angular momentum every `every` steps
+    (drifts relative to the initial values, momentum relative to the sum of
+    m|v|), median / p99 force error against FP64 direct sums at `probes`
+    probes at the start and the end, and the particle-steps/s of the steps
+    themselves (log points excluded)."""
+    import dataclasses as dc
+
+    import numpy as np
+    import torch
+
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
+
+    rt = ParallelTreeRuntime(gpu)
+    s0 = bodies_to_state(scenarios.binary_encounter(n, seed=11, eps=0.005))
+    probe_idx = np.linspace(0, n - 1, probes).astype(np.uint32)
+    stream = torch.cuda.ExternalStream(gpu.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    out = {"workload": f"binary disc encounter N={n}, eps 0.005, dt 5e-4, compensated two-sum "
+                       f"forces, {steps} steps, FP64 invariants every {every} steps",
+           "thetas": {}}
+    for theta in thetas:
+        cfg = Config(theta=theta, softening_kpc=0.005, g=1.0, bucket=1, max_depth=48,
+                     compensated=True)
+        cfg_pot = dc.replace(cfg, potential=True)
+        ev, _ = gpu.create_evolving_state_records(s0)
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg_pot)  # boundary solve, with the potential for E0
+        err0 = gpu.probe_error(ev, cfg, probe_idx)
+        c0 = gpu.conservation(ev)
+        drift = {"energy": 0.0, "momentum": 0.0, "lz": 0.0}
+        step_ms = 0.0
+        done = 0
+        while done < steps:
+            k = min(every, steps - done)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            rt.step(gpu, ev, tree, cfg, 5e-4, k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            step_ms += e0.elapsed_time(e1)
+            done += k
+            # the same tree and positions: this force reproduces the boundary
+            # accelerations bit for bit and adds the potential
+            rt.force(gpu, ev, tree, cfg_pot)
+            c = gpu.conservation(ev)
+            drift["energy"] = max(drift["energy"],
+                                  abs(c["energy"] - c0["energy"]) / abs(c0["energy"]))
+            drift["momentum"] = max(drift["momentum"],
+                                    float(np.hypot(c["px"] - c0["px"], c["py"] - c0["py"]))
+                                    / c0["mass_speed_scale"])
+            drift["lz"] = max(drift["lz"], abs(c["lz"] - c0["lz"]) / abs(c0["lz"]))
+        err1 = gpu.probe_error(ev, cfg, probe_idx)
+        out["thetas"][str(theta)] = {
+            "value": n * steps / (step_ms * 1e-3), "unit": METRIC,
+            "ms_per_step": step_ms / steps, "force_error_start": err0,
+            "force_error_end": err1, "max_relative_drift": drift,
+            "initial": {k: c0[k] for k in ("energy", "px", "py", "lz", "mass")}}
+        tree.close()
+        ev.close()
+    return out
 
 
 def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps: int = 5,
@@ -568,6 +647,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the mixed-size batched workload leg")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload leg")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the precision-form leg (binary encounter, N=2^22)")
+    ap.add_argument("--precision-steps", type=int, default=500)
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -397,3 +397,26 @@ def test_state_upload_and_readback_checks(gpu, oracle):
     assert rc == _lib.BH_NONFINITE
     assert f"at {first}" in _lib.last_error()
     assert np.array_equal(out.view(np.float32).reshape(-1, 8), want)
+
+
+def test_force_after_step_reproduces_step_accelerations(gpu, rt):
+    """A force on the tree a step left behind (same positions) recomputes the
+    step's closing accelerations bit for bit, with or without the potential
+    and the statistics: the precision leg logs energies this way."""
+    import dataclasses as dc
+    bodies = scenarios.binary_encounter(20000, seed=3)
+    cfg = Config(theta=0.5, softening_kpc=0.005, g=1.0, bucket=1, compensated=True)
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    rt.step(gpu, ev, tree, cfg, 5e-4, 7)
+    a_step, _ = gpu.read_evolving_accelerations_f32(ev)
+    rt.force(gpu, ev, tree, dc.replace(cfg, potential=True))
+    a_pot, _ = gpu.read_evolving_accelerations_f32(ev)
+    assert np.array_equal(a_step.view(np.uint32), a_pot.view(np.uint32))
+    rt.force(gpu, ev, tree, dc.replace(cfg, force_stats=False))
+    a_plain, _ = gpu.read_evolving_accelerations_f32(ev)
+    assert np.array_equal(a_step.view(np.uint32), a_plain.view(np.uint32))
+    c = gpu.conservation(ev)
+    assert c["potential"] < 0.0 and np.isfinite(c["energy"])
