@@ -78,6 +78,11 @@ class BhBuildTiming(C.Structure):
                 ("topology_seconds", C.c_double), ("aggregate_seconds", C.c_double)]
 
 
+class BhTuning(C.Structure):
+    _fields_ = [("radix_bits", C.c_uint32), ("traverse_warps", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
 class BhForceStats(C.Structure):
     _fields_ = [("visited_nodes", C.c_uint64), ("approximated_cells", C.c_uint64),
                 ("direct_terms", C.c_uint64), ("exact_mac_fallbacks", C.c_uint64),
@@ -125,6 +130,8 @@ SIGNATURES = {
     "galaxy_bh_batch_solve": (C.c_int, [_P, _P]),
     "galaxy_bh_batch_step": (C.c_int, [_P, _P, C.POINTER(C.c_double), _U32]),
     "galaxy_bh_batch_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "galaxy_bh_batch_tune": (C.c_int, [_P, _P]),
+    "galaxy_bh_tree_tune": (C.c_int, [_P, _P]),
     "galaxy_bh_batch_footprint": (C.c_int, [_P, C.POINTER(BhConfig), _U32,
                                             C.POINTER(C.c_uint64)]),
 }

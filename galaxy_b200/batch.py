@@ -47,6 +47,12 @@ class Batch:
                                                d.ctypes.data_as(C.POINTER(C.c_double)),
                                                int(steps)))
 
+    def tune(self, radix_bits: int = 8, traverse_warps: int = 8) -> None:
+        """Launch-shape knobs (sort digit width, warps per traversal block);
+        results are bit-identical under every setting."""
+        t = _lib.BhTuning(int(radix_bits), int(traverse_warps), (C.c_uint32 * 2)(0, 0))
+        check(_lib.load().galaxy_bh_batch_tune(self._h.p, C.byref(t)))
+
     def arena_bytes(self) -> int:
         v = C.c_uint64()
         check(_lib.load().galaxy_bh_batch_bytes(self._h.p, C.byref(v)))

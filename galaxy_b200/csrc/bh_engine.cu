@@ -608,7 +608,7 @@ struct ArenaPlan {
 
 static ArenaPlan plan_arena(const Layout& L, uint32_t nsims) {
     ArenaPlan a;
-    a.control = align256(4ull * nsims * 4 + 4ull * nsims * kRadixPasses * kRadixDigits + 4ull * 8 +
+    a.control = align256(4ull * nsims * 4 + 4ull * nsims * kRadixPasses * kRadixDigits + 4ull * 16 +
                          4ull * kRadixPasses * L.ntiles * kRadixDigits) +
                 align256(8ull * L.nscan_tiles);
     a.sims = align256(sizeof(SimDesc) * nsims);
@@ -703,7 +703,7 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.hist = (uint32_t*)cp;
     cp += 4ull * count * kRadixPasses * kRadixDigits;
     bb.counters = (uint32_t*)cp;
-    cp += 4ull * 8;
+    cp += 4ull * 16;
     bb.sort_flags = (uint32_t*)cp;
     cp += 4ull * kRadixPasses * L.ntiles * kRadixDigits;
     bb.scan_flags = (unsigned long long*)((char*)b->control +
@@ -734,6 +734,8 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.ntiles = L.ntiles;
     bb.nscan_tiles = L.nscan_tiles;
     bb.cell_capacity = (uint32_t)L.cells;
+    bb.radix_bits = 8;
+    bb.trav_warps = 8;
 
     b->h_sims.resize(count);
     b->h_chunk_sim.assign(L.nchunks, kNone);
@@ -948,6 +950,8 @@ static int tree_fit(bh_tree* tree, const bh_config* cfg) {
     if (cell_bound(tree->st->n, *cfg) <= tree->batch->cell_capacity) return BH_OK;
     Batch* nb = nullptr;
     if ((rc = batch_build(tree->dev, &tree->st, cfg, 1, &nb))) return rc;
+    nb->bb.radix_bits = tree->batch->bb.radix_bits;  // keep the tree's tuning
+    nb->bb.trav_warps = tree->batch->bb.trav_warps;
     delete tree->batch;
     tree->batch = nb;
     tree->built = false;
@@ -1270,6 +1274,32 @@ extern "C" int galaxy_bh_batch_step(bh_device* dev, bh_batch* batch, const doubl
     if (nsteps == 0) return BH_OK;
     if ((rc = upload_sims(b))) return rc;
     return run_graphs(b, nsteps);
+}
+
+// Installs launch-shape knobs; the next step re-captures its graphs.
+static int apply_tuning(Batch* b, const bh_tuning* t) {
+    if (!t) return set_error(BH_INVALID_ARG, "null argument");
+    if (t->radix_bits != 4 && t->radix_bits != 8)
+        return set_error(BH_INVALID_ARG, "radix_bits must be 4 or 8, got %u", t->radix_bits);
+    if (t->traverse_warps != 4 && t->traverse_warps != 8)
+        return set_error(BH_INVALID_ARG, "traverse_warps must be 4 or 8, got %u",
+                         t->traverse_warps);
+    if (t->radix_bits != b->bb.radix_bits || t->traverse_warps != b->bb.trav_warps) {
+        b->bb.radix_bits = t->radix_bits;
+        b->bb.trav_warps = t->traverse_warps;
+        b->graph_flags = 0xffffffffu;  // graphs hold the old launch shapes
+    }
+    return BH_OK;
+}
+
+extern "C" int galaxy_bh_batch_tune(bh_batch* batch, const bh_tuning* tuning) {
+    if (!batch) return set_error(BH_INVALID_ARG, "null batch");
+    return apply_tuning(batch->batch, tuning);
+}
+
+extern "C" int galaxy_bh_tree_tune(bh_tree* tree, const bh_tuning* tuning) {
+    if (!tree) return set_error(BH_INVALID_ARG, "null tree");
+    return apply_tuning(tree->batch, tuning);
 }
 
 extern "C" int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes) {

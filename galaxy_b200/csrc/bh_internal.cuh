@@ -86,10 +86,12 @@ struct BatchBuffers {
     uint32_t ntiles;
     uint32_t nscan_tiles;
     uint32_t cell_capacity;
+    uint32_t radix_bits;   // 8 (4 passes) or 4 (8 passes); results do not depend on it
+    uint32_t trav_warps;   // warps per traversal block, 8 or 4; results do not depend on it
     // zeroed once per rebuild (one memset): control block
     uint32_t* minmax;      // nsims * 4 (atomicMax of encoded floats; mins stored inverted)
     uint32_t* hist;        // nsims * 4 * 256
-    uint32_t* counters;    // 8: radix tile counters (4), scan tile counter
+    uint32_t* counters;    // 16: radix tile counters (one per pass, <= 8), scan tile counter [8]
     uint32_t* sort_flags;  // 4 * ntiles * 256
     unsigned long long* scan_flags;  // nscan_tiles
     // transient per rebuild

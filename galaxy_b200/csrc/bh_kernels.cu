@@ -278,16 +278,21 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
 
 // ============================================================== morton ====
 
+constexpr uint32_t kHistStride = kRadixPasses * kRadixDigits;  // histogram words per sim
+
 // One block per radix tile: Morton codes of the tile's bodies (resident
-// order) plus the tile's contribution to the four digit histograms.
+// order) plus the tile's contribution to the digit histograms of every pass
+// of a BITS-wide LSD sort (hist[sim][pass * 2^BITS + digit]).
+template <int BITS>
 __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restrict__ sims,
                                                          const Tile* __restrict__ tiles,
                                                          const uint32_t* __restrict__ minmax,
                                                          uint32_t* __restrict__ keys,
                                                          uint32_t* hist, SimOut* simout) {
-    __shared__ uint32_t sh[kRadixPasses][kRadixDigits];
-    for (int k = threadIdx.x; k < kRadixPasses * kRadixDigits; k += kSortThreads)
-        (&sh[0][0])[k] = 0;
+    constexpr int kPasses = 32 / BITS;
+    constexpr uint32_t kDig = 1u << BITS;
+    __shared__ uint32_t sh[kPasses * kDig];
+    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kSortThreads) sh[k] = 0;
     __syncthreads();
     const Tile t = tiles[blockIdx.x];
     const SimDesc& sd = sims[t.sim];
@@ -307,14 +312,14 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
                                           quantize_axis((double)xy.y, rb.cy, rb.half));
             keys[p] = code;
 #pragma unroll
-            for (int pass = 0; pass < kRadixPasses; ++pass)
-                atomicAdd(&sh[pass][(code >> (8 * pass)) & 255u], 1u);
+            for (int pass = 0; pass < kPasses; ++pass)
+                atomicAdd(&sh[pass * kDig + ((code >> (BITS * pass)) & (kDig - 1u))], 1u);
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kRadixPasses * kRadixDigits; k += kSortThreads) {
-        const uint32_t c = (&sh[0][0])[k];
-        if (c) atomicAdd(&hist[(size_t)t.sim * kRadixPasses * kRadixDigits + k], c);
+    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kSortThreads) {
+        const uint32_t c = sh[k];
+        if (c) atomicAdd(&hist[(size_t)t.sim * kHistStride + k], c);
     }
 }
 
@@ -325,34 +330,36 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = (1u << 30) - 1u;
 
-// One stable 8-bit LSD pass over every simulation's keys.  Tiles never cross
+// One stable BITS-wide LSD pass (BITS = 8: 4 passes, 4: 8 passes) over every
+// simulation's keys.  Tiles never cross
 // simulations; within a simulation, tile order is key order and the
 // decoupled look-back adds the digit counts of the preceding tiles.  Items
 // are ranked warp by warp in key order (match_any peers), so equal digits keep
 // their input order: the permutation equals a stable sort by code, as
 // Rust's sort_by_key (nbody/src/flat.rs:233-234).
-template <int PASS, bool LAST>
+template <int BITS, int PASS, bool LAST>
 __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     const SimDesc* __restrict__ sims, const Tile* __restrict__ tiles, uint32_t* tile_counter,
     const uint32_t* __restrict__ hist, uint32_t* flags, const uint32_t* __restrict__ keys_in,
     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, float4* __restrict__ sbody, uint32_t* err) {
+    constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t s_tile;
-    __shared__ uint32_t s_whist[8][kRadixDigits];
-    __shared__ uint32_t s_tprefix[kRadixDigits];
-    __shared__ uint32_t s_out[kRadixDigits];
+    __shared__ uint32_t s_whist[8][kDig];
+    __shared__ uint32_t s_tprefix[kDig];
+    __shared__ uint32_t s_out[kDig];
     __shared__ uint32_t s_keys[kTile];
     __shared__ uint32_t s_vals[kTile];
     __shared__ uint32_t s_scan[8];
 
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
-    for (int k = threadIdx.x; k < 8 * kRadixDigits; k += kSortThreads) (&s_whist[0][0])[k] = 0;
+    for (int k = threadIdx.x; k < 8 * (int)kDig; k += kSortThreads) (&s_whist[0][0])[k] = 0;
     __syncthreads();
     const uint32_t t = s_tile;
     const Tile tl = tiles[t];
     const SimDesc& sd = sims[tl.sim];
-    const uint32_t shift = 8u * PASS;
+    const uint32_t shift = (uint32_t)BITS * PASS;
     const uint32_t lt_mask = (1u << lane) - 1u;
 
     uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
@@ -368,7 +375,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = warp * 256u + r * 32u + lane;
         const bool valid = idx < tl.count;
-        const uint32_t d = valid ? ((key[r] >> shift) & 255u) : (256u + lane);
+        const uint32_t d = valid ? ((key[r] >> shift) & (kDig - 1u)) : (kDig + lane);
         const uint32_t peers = __match_any_sync(kFull, d);
         const uint32_t leader = __ffs(peers) - 1u;
         uint32_t b = 0;
@@ -382,20 +389,24 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     }
     __syncthreads();
 
-    // Thread d owns digit d: warp offsets, tile count, look-back, bases.
+    // Thread d < 2^BITS owns digit d: warp offsets, tile count, look-back,
+    // bases (the other threads feed zeros to the block scans).
     const uint32_t d = threadIdx.x;
+    const bool owner = d < kDig;
     uint32_t run = 0;
+    if (owner) {
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        const uint32_t c = s_whist[w][d];
-        s_whist[w][d] = run;
-        run += c;
+        for (int w = 0; w < 8; ++w) {
+            const uint32_t c = s_whist[w][d];
+            s_whist[w][d] = run;
+            run += c;
+        }
     }
     const bool first = (t == sd.first_tile);
-    uint32_t* my_flag = flags + (size_t)t * kRadixDigits + d;
-    atomicExch(my_flag, (first ? kFlagInc : kFlagAgg) | run);
+    uint32_t* my_flag = flags + (size_t)t * kDig + d;
+    if (owner) atomicExch(my_flag, (first ? kFlagInc : kFlagAgg) | run);
     uint32_t excl = 0;
-    if (!first) {
+    if (owner && !first) {
         // look back kLookWindow predecessors per round trip: add aggregates
         // up to the nearest inclusive prefix; re-poll from the first tile
         // that has not published yet.  The simulation's first tile is
@@ -407,7 +418,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
 #pragma unroll
             for (int j = 0; j < kLookWindow; ++j)
                 f[j] = tp >= sd.first_tile + j
-                           ? ld_volatile(flags + (size_t)(tp - j) * kRadixDigits + d)
+                           ? ld_volatile(flags + (size_t)(tp - j) * kDig + d)
                            : 0u;
             bool done = false;
             int used = 0;
@@ -430,17 +441,19 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
         atomicExch(my_flag, kFlagInc | (excl + run));
     }
     uint32_t tot;
-    const uint32_t h = hist[((size_t)tl.sim * kRadixPasses + PASS) * kRadixDigits + d];
+    const uint32_t h = owner ? hist[(size_t)tl.sim * kHistStride + PASS * kDig + d] : 0u;
     const uint32_t gex = block_exclusive_scan_256(h, &tot, s_scan);
     const uint32_t tex = block_exclusive_scan_256(run, &tot, s_scan);
-    s_tprefix[d] = tex;
-    s_out[d] = sd.off + gex + excl - tex;
+    if (owner) {
+        s_tprefix[d] = tex;
+        s_out[d] = sd.off + gex + excl - tex;
+    }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = warp * 256u + r * 32u + lane;
         if (idx < tl.count) {
-            const uint32_t dg = (key[r] >> shift) & 255u;
+            const uint32_t dg = (key[r] >> shift) & (kDig - 1u);
             const uint32_t slot = s_tprefix[dg] + s_whist[warp][dg] + rank[r];
             s_keys[slot] = key[r];
             s_vals[slot] = val[r];
@@ -453,7 +466,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
         if (slot < tl.count) {
             const uint32_t kk = s_keys[slot];
             const uint32_t vv = s_vals[slot];
-            const uint32_t dest = s_out[(kk >> shift) & 255u] + slot;
+            const uint32_t dest = s_out[(kk >> shift) & (kDig - 1u)] + slot;
             keys_out[dest] = kk;
             vals_out[dest] = vv;
             if (LAST) {
@@ -1084,18 +1097,19 @@ constexpr uint32_t kTravStack = 17u * 32u;
 // Interaction list: flushed once it holds >= 32 entries; a step adds <= 32.
 constexpr uint32_t kTravList = 64u;
 
-template <bool COMP, bool POT, bool STATS>
-__global__ void __launch_bounds__(kTravWarps * 32, GBH_TRAVERSE_MIN_BLOCKS) k_traverse(
+template <bool COMP, bool POT, bool STATS, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWarps / WARPS)
+    k_traverse(
     const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
     const uint32_t* __restrict__ chunk_sim, uint32_t nchunks, const float4* __restrict__ sbody,
     const CellRec* __restrict__ groups, const double4* __restrict__ cell_d, uint32_t capacity,
     unsigned long long* stats, uint32_t* err) {
-    __shared__ uint2 s_stack[kTravWarps][kTravStack];  // (node group, lane mask)
-    __shared__ float4 s_list[kTravWarps][kTravList];   // (com_x, com_y, G*m, lane mask bits)
-    __shared__ uint4 s_mix[kTravWarps][32];  // mixed slots: (group, slot, lane mask, opened)
+    __shared__ uint2 s_stack[WARPS][kTravStack];  // (node group, lane mask)
+    __shared__ float4 s_list[WARPS][kTravList];   // (com_x, com_y, G*m, lane mask bits)
+    __shared__ uint4 s_mix[WARPS][32];  // mixed slots: (group, slot, lane mask, opened)
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
-    const uint32_t chunk = blockIdx.x * kTravWarps + warp;
+    const uint32_t chunk = blockIdx.x * WARPS + warp;
     if (chunk >= nchunks) return;
     const uint32_t s = chunk_sim[chunk];
     if (s == kNone) return;
@@ -1637,31 +1651,43 @@ cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s) {
 }
 
 cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s) {
-    k_morton<<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a, b.hist,
-                                               b.simout);
+    if (b.radix_bits == 4)
+        k_morton<4><<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a,
+                                                      b.hist, b.simout);
+    else
+        k_morton<8><<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a,
+                                                      b.hist, b.simout);
     return cudaGetLastError();
 }
 
+// Passes alternate a -> b -> a ...; an even pass count leaves the sorted keys
+// in keys_a / vals_a, and the last pass also gathers the sorted bodies.
+template <int BITS, int PASS>
+static void radix_passes(const BatchBuffers& b, cudaStream_t s) {
+    constexpr int kPasses = 32 / BITS;
+    const size_t fstride = (size_t)b.ntiles << BITS;
+    const bool even = (PASS % 2) == 0;
+    const uint32_t* kin = even ? b.keys_a : b.keys_b;
+    const uint32_t* vin = even ? b.vals_a : b.vals_b;
+    uint32_t* kout = even ? b.keys_b : b.keys_a;
+    uint32_t* vout = even ? b.vals_b : b.vals_a;
+    k_radix_pass<BITS, PASS, PASS == kPasses - 1><<<b.ntiles, kSortThreads, 0, s>>>(
+        b.sims, b.tiles, b.counters + PASS, b.hist, b.sort_flags + PASS * fstride, kin,
+        PASS == 0 ? nullptr : vin, kout, vout, b.sbody, b.err);
+    if constexpr (PASS + 1 < kPasses) radix_passes<BITS, PASS + 1>(b, s);
+}
+
 cudaError_t launch_radix(const BatchBuffers& b, cudaStream_t s) {
-    const size_t fstride = (size_t)b.ntiles * kRadixDigits;
-    k_radix_pass<0, false><<<b.ntiles, kSortThreads, 0, s>>>(
-        b.sims, b.tiles, b.counters + 0, b.hist, b.sort_flags, b.keys_a, nullptr, b.keys_b,
-        b.vals_b, b.sbody, b.err);
-    k_radix_pass<1, false><<<b.ntiles, kSortThreads, 0, s>>>(
-        b.sims, b.tiles, b.counters + 1, b.hist, b.sort_flags + fstride, b.keys_b, b.vals_b,
-        b.keys_a, b.vals_a, b.sbody, b.err);
-    k_radix_pass<2, false><<<b.ntiles, kSortThreads, 0, s>>>(
-        b.sims, b.tiles, b.counters + 2, b.hist, b.sort_flags + 2 * fstride, b.keys_a, b.vals_a,
-        b.keys_b, b.vals_b, b.sbody, b.err);
-    k_radix_pass<3, true><<<b.ntiles, kSortThreads, 0, s>>>(
-        b.sims, b.tiles, b.counters + 3, b.hist, b.sort_flags + 3 * fstride, b.keys_b, b.vals_b,
-        b.keys_a, b.vals_a, b.sbody, b.err);
+    if (b.radix_bits == 4)
+        radix_passes<4, 0>(b, s);
+    else
+        radix_passes<8, 0>(b, s);
     return cudaGetLastError();
 }
 
 cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
     k_count_scan<<<b.nscan_tiles, kScanThreads, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.keys_a,
-                                                        b.base, b.counters + 4, b.scan_flags,
+                                                        b.base, b.counters + 8, b.scan_flags,
                                                         b.err);
     return cudaGetLastError();
 }
@@ -1690,11 +1716,12 @@ cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
+template <int WARPS>
+static void traverse_launch(const BatchBuffers& b, bool compensated, bool potential, bool stats,
                             cudaStream_t s) {
-    const uint32_t blocks = (b.nchunks + kTravWarps - 1) / kTravWarps;
+    const uint32_t blocks = (b.nchunks + WARPS - 1) / WARPS;
 #define GBH_TRAVERSE(C, P, S)                                                                   \
-    k_traverse<C, P, S><<<blocks, kTravWarps * 32, 0, s>>>(                                  \
+    k_traverse<C, P, S, WARPS><<<blocks, WARPS * 32, 0, s>>>(                                \
         b.sims, b.simout, b.chunk_sim, b.nchunks, b.sbody, b.groups, b.cell_d, b.cell_capacity, \
         b.force_stats, b.err)
     if (stats) {
@@ -1711,6 +1738,14 @@ cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potent
         }
     }
 #undef GBH_TRAVERSE
+}
+
+cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
+                            cudaStream_t s) {
+    if (b.trav_warps == 4)
+        traverse_launch<4>(b, compensated, potential, stats, s);
+    else
+        traverse_launch<kTravWarps>(b, compensated, potential, stats, s);
     return cudaGetLastError();
 }
 

@@ -508,6 +508,12 @@ class ParallelTreeRuntime:
         return ParallelGpuTreeEvidence(meta, entries, bodies, cells, len(cells),
                                        int(leaf.sum()), int(cells["range_depth"][:, 2].max()))
 
+    def tune(self, tree: ParallelGpuTree, radix_bits: int = 8, traverse_warps: int = 8) -> None:
+        """Launch-shape knobs of this tree's steps (no counterpart in the
+        reference); results are bit-identical under every setting."""
+        t = _lib.BhTuning(int(radix_bits), int(traverse_warps), (C.c_uint32 * 2)(0, 0))
+        check(_lib.load().galaxy_bh_tree_tune(tree.handle, C.byref(t)))
+
     def buffer_bytes(self, tree: ParallelGpuTree) -> int:
         v = C.c_uint64()
         check(_lib.load().galaxy_bh_tree_buffer_bytes(tree.handle, C.byref(v)))

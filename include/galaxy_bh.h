@@ -267,6 +267,21 @@ int galaxy_bh_batch_solve(bh_device* dev, bh_batch* batch);
  * re-formed from states that were already stepping. */
 int galaxy_bh_batch_step(bh_device* dev, bh_batch* batch, const double* dts, uint32_t nsteps);
 int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
+
+/* ---- launch-shape tuning --------------------------------------------------
+ * No reference counterpart (the reference's WGSL dispatch shapes are fixed).
+ * Knobs the autotuner (galaxy_b200/autotune.py) picks per batch or tree;
+ * neither changes any result bit: the sort is the same stable permutation
+ * at either digit width and each traversal warp does the same work at
+ * either block size.  Takes effect at the next launch (graphs are
+ * re-captured).  Leaf size, the third knob, is bh_config.bucket. */
+typedef struct {
+    uint32_t radix_bits;      /* 8 (default): 4 sort passes; 4: 8 passes */
+    uint32_t traverse_warps;  /* 8 (default) or 4 warps per traversal block */
+    uint32_t reserved[2];
+} bh_tuning;
+int galaxy_bh_batch_tune(bh_batch* batch, const bh_tuning* tuning);
+int galaxy_bh_tree_tune(bh_tree* tree, const bh_tuning* tuning);
 /* Device bytes a batch of these sizes/configs would need (admission). */
 int galaxy_bh_batch_footprint(const uint32_t* counts, const bh_config* cfgs, uint32_t count,
                               uint64_t* bytes);

@@ -67,3 +67,55 @@ def test_batch_solve_matches_plain_force(gpu):
         rt.force(gpu, ev, tree, cfg)
         assert np.array_equal(gpu.read_evolving_accelerations_f32(states[k])[0],
                               gpu.read_evolving_accelerations_f32(ev)[0])
+
+
+def test_launch_tuning_changes_no_bit(gpu):
+    """4-bit vs 8-bit sort digits and 4 vs 8 traversal warps per block give
+    the same tree, accelerations and trajectory, bit for bit, on the plain
+    path and in a batch."""
+    rt = ParallelTreeRuntime(gpu)
+    bodies = scenarios.binary_encounter(30000, seed=21)
+    cfg = Config(theta=0.5, softening_kpc=0.005, g=1.0, bucket=1)
+    results = []
+    for bits, warps in ((8, 8), (4, 8), (8, 4), (4, 4)):
+        ev, _ = gpu.create_evolving_state(bodies)
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.tune(tree, bits, warps)
+        rt.rebuild(gpu, ev, tree, cfg)
+        evid = rt.read_evidence(gpu, tree)
+        rt.force(gpu, ev, tree, cfg)
+        a0 = gpu.read_evolving_accelerations_f32(ev)[0]
+        rt.step(gpu, ev, tree, cfg, 5e-4, 3)
+        results.append((evid.entries.tobytes(), evid.cells.tobytes(), a0.tobytes(),
+                        gpu.read_evolving_state_records(ev)[0].tobytes()))
+        tree.close()
+        ev.close()
+    assert all(r == results[0] for r in results[1:])
+    # batched: same members, both knob settings
+    states = []
+    for bits, warps in ((8, 8), (4, 4)):
+        evs = [gpu.create_evolving_state(scenarios.make(n, c, s))[0] for n, c, s, _ in MEMBERS]
+        b = Batch(gpu, evs, [m[3] for m in MEMBERS])
+        b.tune(bits, warps)
+        b.solve()
+        b.step(DTS, STEPS)
+        states.append([gpu.read_evolving_state_records(e)[0].tobytes() for e in evs])
+        b.close()
+    assert states[0] == states[1]
+
+
+def test_autotune_batch_picks_admissible_settings(gpu):
+    from galaxy_b200.autotune import LEAF_SIZES, size_class, tune_batch
+    rng = np.random.default_rng(5)
+    sizes = [int(2 ** rng.uniform(10, 15)) for _ in range(10)]
+    evs = [gpu.create_evolving_state(scenarios.make("exponential_disc", n, 100 + i))[0]
+           for i, n in enumerate(sizes)]
+    cfgs = [Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)] * len(evs)
+    before = [gpu.read_evolving_state_records(e)[0].tobytes() for e in evs]
+    t = tune_batch(gpu, evs, cfgs, dt=1e-3, steps=2, probes=128)
+    assert set(t.leaf_by_class) == {size_class(n) for n in sizes}
+    assert all(v in LEAF_SIZES for v in t.leaf_by_class.values())
+    assert t.radix_bits in (4, 8) and t.traverse_warps in (4, 8)
+    assert t.trials[-1][0] == "best" and t.trials[-1][2] > 0
+    # tuning ran on copies: the caller's states are untouched
+    assert before == [gpu.read_evolving_state_records(e)[0].tobytes() for e in evs]
