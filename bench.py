@@ -503,7 +503,7 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
     another (the same engine, tree per simulation)."""
     import torch
 
-    from galaxy_b200 import scenarios
+    from galaxy_b200 import autotune, scenarios
     from galaxy_b200.batch import Batch
     from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
     plan = scenarios.mixed_batch(count, 10, 18, seed=2024)
@@ -516,17 +516,33 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
     stream = torch.cuda.ExternalStream(gpu.stream_ptr())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    batch = Batch(gpu, states, [cfg] * len(states))
-    batch.solve()
-    batch.step(1e-3, max(warmup, 3))
-    torch.cuda.synchronize()
-    e0.record(stream)
-    batch.step(1e-3, steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    b_ms = e0.elapsed_time(e1)
-    arena = batch.arena_bytes()
-    batch.close()
+    # autotuner (untimed, on copies of the states): leaf size per size class,
+    # sort digit width, traversal warps per block
+    tuning = autotune.tune_batch(gpu, states, [cfg] * len(states), dt=1e-3, steps=2,
+                                 probes=128)
+    tuned_cfgs = tuning.configs([s.count for s in states], [cfg] * len(states))
+
+    def timed(cfgs, bits, warps, run_states):
+        batch = Batch(gpu, run_states, cfgs)
+        batch.tune(bits, warps)
+        batch.solve()
+        batch.step(1e-3, max(warmup, 3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        batch.step(1e-3, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        arena = batch.arena_bytes()
+        batch.close()
+        return ms, arena
+
+    untuned_states = [gpu.create_evolving_state_records(gpu.read_evolving_state_records(s)[0])[0]
+                      for s in states]
+    u_ms, _ = timed([cfg] * len(states), 8, 8, untuned_states)
+    for s in untuned_states:
+        s.close()
+    b_ms, arena = timed(tuned_cfgs, tuning.radix_bits, tuning.traverse_warps, states)
     # plain path, simulation after simulation (a prefix of the plan when
     # plain_sims is set; the rate is per body-step either way)
     rt = ParallelTreeRuntime(gpu)
@@ -553,9 +569,13 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
     batched = total * steps / (b_ms * 1e-3)
     plain = p_bodies * plain_steps / (p_ms * 1e-3)
     return {"workload": f"{count} sims, N log-uniform [2^10, 2^18], mixed scenarios, "
-                        "eps 0.01, theta 0.5, bucket 1, dt 1e-3",
+                        "eps 0.01, theta 0.5, dt 1e-3, autotuned leaf size / sort digits / "
+                        "traversal warps",
             "bodies": total, "steps": steps, "ms_per_step": b_ms / steps,
             "value": batched, "unit": METRIC, "arena_bytes": arena,
+            "tuning": tuning.as_dict(), "tuning_force_error_median": tuning.errors,
+            "untuned": {"value": total * steps / (u_ms * 1e-3), "ms_per_step": u_ms / steps,
+                        "settings": "leaf size 1, 8-bit digits, 8 traversal warps"},
             "plain_serial": {"value": plain, "steps": plain_steps, "sims": len(sims),
                              "ms_per_step": p_ms / plain_steps},
             "speedup_vs_plain": batched / plain}

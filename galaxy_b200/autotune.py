@@ -38,6 +38,7 @@ class Tuning:
     radix_bits: int = 8
     traverse_warps: int = 8
     trials: list = field(default_factory=list)  # (knob, value, ms per step, accepted)
+    errors: dict = field(default_factory=dict)  # "2^class" -> {leaf: median force error}
 
     def bucket_for(self, n: int, default: int = 1) -> int:
         return int(self.leaf_by_class.get(size_class(n), default))
@@ -154,7 +155,10 @@ def tune_batch(gpu, states, configs, dt: float, steps: int = 3, probes: int = 25
         return class_error(cls, leaf) <= max_error_ratio * class_error(cls, 1)
 
     start = Tuning({c: 1 for c in classes})
-    return coordinate_search(start, classes, measure, admissible)
+    best = coordinate_search(start, classes, measure, admissible)
+    for (cls, leaf), e in sorted(errors.items()):
+        best.errors.setdefault(f"2^{cls}", {})[leaf] = e
+    return best
 
 
 def tune_tree(gpu, rt, state, tree, config, dt: float, steps: int = 5) -> Tuning:
