@@ -539,7 +539,7 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
 
     untuned_states = [gpu.create_evolving_state_records(gpu.read_evolving_state_records(s)[0])[0]
                       for s in states]
-    u_ms, _ = timed([cfg] * len(states), 8, 8, untuned_states)
+    u_ms, _ = timed([cfg] * len(states), 8, 4, untuned_states)
     for s in untuned_states:
         s.close()
     b_ms, arena = timed(tuned_cfgs, tuning.radix_bits, tuning.traverse_warps, states)
@@ -575,7 +575,7 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
             "value": batched, "unit": METRIC, "arena_bytes": arena,
             "tuning": tuning.as_dict(), "tuning_force_error_median": tuning.errors,
             "untuned": {"value": total * steps / (u_ms * 1e-3), "ms_per_step": u_ms / steps,
-                        "settings": "leaf size 1, 8-bit digits, 8 traversal warps"},
+                        "settings": "leaf size 1, 8-bit digits, 4 traversal warps (defaults)"},
             "plain_serial": {"value": plain, "steps": plain_steps, "sims": len(sims),
                              "ms_per_step": p_ms / plain_steps},
             "speedup_vs_plain": batched / plain}

@@ -5,7 +5,7 @@ Picks, by timing short runs of the caller's own workload on the device:
 * the leaf size (``Config.bucket``, one of 1, 4, 8, 16) per simulation size
   class, so the leaf size is a pure function of N once tuned;
 * the sort digit width (8 or 4 bits) and the warps per traversal block
-  (8 or 4), launch shapes that change no result bit.
+  (4, 8 or 2), launch shapes that change no result bit.
 
 A leaf-size candidate is admitted only if its median force error against FP64
 direct sums (probes of the class's largest simulation) is no worse than the
@@ -23,7 +23,7 @@ import numpy as np
 
 LEAF_SIZES = (1, 4, 8, 16)
 RADIX_BITS = (8, 4)
-TRAVERSE_WARPS = (8, 4)
+TRAVERSE_WARPS = (4, 8, 2)
 
 
 def size_class(n: int) -> int:
@@ -36,7 +36,7 @@ def size_class(n: int) -> int:
 class Tuning:
     leaf_by_class: dict = field(default_factory=dict)  # size class -> bucket
     radix_bits: int = 8
-    traverse_warps: int = 8
+    traverse_warps: int = 4
     trials: list = field(default_factory=list)  # (knob, value, ms per step, accepted)
     errors: dict = field(default_factory=dict)  # "2^class" -> {leaf: median force error}
 

@@ -47,7 +47,7 @@ class Batch:
                                                d.ctypes.data_as(C.POINTER(C.c_double)),
                                                int(steps)))
 
-    def tune(self, radix_bits: int = 8, traverse_warps: int = 8) -> None:
+    def tune(self, radix_bits: int = 8, traverse_warps: int = 4) -> None:
         """Launch-shape knobs (sort digit width, warps per traversal block);
         results are bit-identical under every setting."""
         t = _lib.BhTuning(int(radix_bits), int(traverse_warps), (C.c_uint32 * 2)(0, 0))

@@ -735,7 +735,7 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.nscan_tiles = L.nscan_tiles;
     bb.cell_capacity = (uint32_t)L.cells;
     bb.radix_bits = 8;
-    bb.trav_warps = 8;
+    bb.trav_warps = 4;
 
     b->h_sims.resize(count);
     b->h_chunk_sim.assign(L.nchunks, kNone);
@@ -1281,8 +1281,8 @@ static int apply_tuning(Batch* b, const bh_tuning* t) {
     if (!t) return set_error(BH_INVALID_ARG, "null argument");
     if (t->radix_bits != 4 && t->radix_bits != 8)
         return set_error(BH_INVALID_ARG, "radix_bits must be 4 or 8, got %u", t->radix_bits);
-    if (t->traverse_warps != 4 && t->traverse_warps != 8)
-        return set_error(BH_INVALID_ARG, "traverse_warps must be 4 or 8, got %u",
+    if (t->traverse_warps != 2 && t->traverse_warps != 4 && t->traverse_warps != 8)
+        return set_error(BH_INVALID_ARG, "traverse_warps must be 2, 4 or 8, got %u",
                          t->traverse_warps);
     if (t->radix_bits != b->bb.radix_bits || t->traverse_warps != b->bb.trav_warps) {
         b->bb.radix_bits = t->radix_bits;

@@ -87,7 +87,7 @@ struct BatchBuffers {
     uint32_t nscan_tiles;
     uint32_t cell_capacity;
     uint32_t radix_bits;   // 8 (4 passes) or 4 (8 passes); results do not depend on it
-    uint32_t trav_warps;   // warps per traversal block, 8 or 4; results do not depend on it
+    uint32_t trav_warps;   // warps per traversal block, 2, 4 or 8; results do not depend on it
     // zeroed once per rebuild (one memset): control block
     uint32_t* minmax;      // nsims * 4 (atomicMax of encoded floats; mins stored inverted)
     uint32_t* hist;        // nsims * 4 * 256

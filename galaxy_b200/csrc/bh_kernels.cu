@@ -1742,7 +1742,9 @@ static void traverse_launch(const BatchBuffers& b, bool compensated, bool potent
 
 cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
                             cudaStream_t s) {
-    if (b.trav_warps == 4)
+    if (b.trav_warps == 2)
+        traverse_launch<2>(b, compensated, potential, stats, s);
+    else if (b.trav_warps == 4)
         traverse_launch<4>(b, compensated, potential, stats, s);
     else
         traverse_launch<kTravWarps>(b, compensated, potential, stats, s);

@@ -508,7 +508,7 @@ class ParallelTreeRuntime:
         return ParallelGpuTreeEvidence(meta, entries, bodies, cells, len(cells),
                                        int(leaf.sum()), int(cells["range_depth"][:, 2].max()))
 
-    def tune(self, tree: ParallelGpuTree, radix_bits: int = 8, traverse_warps: int = 8) -> None:
+    def tune(self, tree: ParallelGpuTree, radix_bits: int = 8, traverse_warps: int = 4) -> None:
         """Launch-shape knobs of this tree's steps (no counterpart in the
         reference); results are bit-identical under every setting."""
         t = _lib.BhTuning(int(radix_bits), int(traverse_warps), (C.c_uint32 * 2)(0, 0))

@@ -277,7 +277,7 @@ int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
  * re-captured).  Leaf size, the third knob, is bh_config.bucket. */
 typedef struct {
     uint32_t radix_bits;      /* 8 (default): 4 sort passes; 4: 8 passes */
-    uint32_t traverse_warps;  /* 8 (default) or 4 warps per traversal block */
+    uint32_t traverse_warps;  /* 4 (default), 2 or 8 warps per traversal block */
     uint32_t reserved[2];
 } bh_tuning;
 int galaxy_bh_batch_tune(bh_batch* batch, const bh_tuning* tuning);

@@ -14,12 +14,12 @@ def test_size_classes_are_two_octave_bins():
 
 def cost(t: Tuning) -> float:
     # separable model: class 10 prefers leaf 8, class 16 prefers leaf 4,
-    # 4-bit digits are slower, 4 traversal warps are faster
+    # 4-bit digits are slower, 4 traversal warps are fastest
     ms = 10.0
     ms += {1: 3.0, 4: 2.0, 8: 1.0, 16: 1.5}[t.leaf_by_class.get(10, 1)]
     ms += {1: 5.0, 4: 1.0, 8: 2.0, 16: 4.0}[t.leaf_by_class.get(16, 1)]
     ms += 0.0 if t.radix_bits == 8 else 0.7
-    ms += 0.0 if t.traverse_warps == 4 else 0.3
+    ms += {4: 0.0, 8: 0.3, 2: 0.2}[t.traverse_warps]
     return ms
 
 
@@ -27,8 +27,8 @@ def test_coordinate_search_finds_separable_optimum():
     best = coordinate_search(Tuning({10: 1, 16: 1}), [10, 16], cost)
     assert best.leaf_by_class == {10: 8, 16: 4}
     assert best.radix_bits == 8 and best.traverse_warps == 4
-    # baseline + 3 alternatives per class + one per launch knob + the result
-    assert len(best.trials) == 1 + 2 * (len(LEAF_SIZES) - 1) + 2 + 1
+    # baseline + 3 alternatives per class + the other launch-knob values + the result
+    assert len(best.trials) == 1 + 2 * (len(LEAF_SIZES) - 1) + 1 + 2 + 1
     assert best.trials[-1][2] == cost(best)
 
 

@@ -77,7 +77,7 @@ def test_launch_tuning_changes_no_bit(gpu):
     bodies = scenarios.binary_encounter(30000, seed=21)
     cfg = Config(theta=0.5, softening_kpc=0.005, g=1.0, bucket=1)
     results = []
-    for bits, warps in ((8, 8), (4, 8), (8, 4), (4, 4)):
+    for bits, warps in ((8, 8), (4, 8), (8, 4), (4, 4), (8, 2)):
         ev, _ = gpu.create_evolving_state(bodies)
         tree = rt.create_tree(gpu, ev, cfg)
         rt.tune(tree, bits, warps)
@@ -115,7 +115,7 @@ def test_autotune_batch_picks_admissible_settings(gpu):
     t = tune_batch(gpu, evs, cfgs, dt=1e-3, steps=2, probes=128)
     assert set(t.leaf_by_class) == {size_class(n) for n in sizes}
     assert all(v in LEAF_SIZES for v in t.leaf_by_class.values())
-    assert t.radix_bits in (4, 8) and t.traverse_warps in (4, 8)
+    assert t.radix_bits in (4, 8) and t.traverse_warps in (2, 4, 8)
     assert t.trials[-1][0] == "best" and t.trials[-1][2] > 0
     # tuning ran on copies: the caller's states are untouched
     assert before == [gpu.read_evolving_state_records(e)[0].tobytes() for e in evs]
