@@ -12,8 +12,8 @@ namespace gbh {
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kChunk = 32;  // positions per warp chunk; sims start on a chunk boundary
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 8;
-constexpr uint32_t kTile = kSortThreads * kSortItems;  // keys per radix tile (2048)
+constexpr int kSortItems = 16;
+constexpr uint32_t kTile = kSortThreads * kSortItems;  // keys per radix tile (4096)
 constexpr int kRadixDigits = 256;
 constexpr int kRadixPasses = 4;
 constexpr int kScanThreads = 256;

@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        const uint32_t idx = warp * 256u + r * 32u + lane;
+        const uint32_t idx = warp * (kSortItems * 32u) + r * 32u + lane;
         const bool valid = idx < tl.count;
         const uint32_t p = tl.start + idx;
         key[r] = valid ? keys_in[p] : 0u;
@@ -373,7 +373,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     }
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        const uint32_t idx = warp * 256u + r * 32u + lane;
+        const uint32_t idx = warp * (kSortItems * 32u) + r * 32u + lane;
         const bool valid = idx < tl.count;
         const uint32_t d = valid ? ((key[r] >> shift) & (kDig - 1u)) : (kDig + lane);
         const uint32_t peers = __match_any_sync(kFull, d);
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        const uint32_t idx = warp * 256u + r * 32u + lane;
+        const uint32_t idx = warp * (kSortItems * 32u) + r * 32u + lane;
         if (idx < tl.count) {
             const uint32_t dg = (key[r] >> shift) & (kDig - 1u);
             const uint32_t slot = s_tprefix[dg] + s_whist[warp][dg] + rank[r];
