@@ -131,6 +131,7 @@ SIGNATURES = {
     "galaxy_bh_batch_step": (C.c_int, [_P, _P, C.POINTER(C.c_double), _U32]),
     "galaxy_bh_batch_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "galaxy_bh_batch_tune": (C.c_int, [_P, _P]),
+    "galaxy_bh_tree_footprint": (C.c_int, [C.c_uint32, _P, C.POINTER(C.c_uint64)]),
     "galaxy_bh_tree_tune": (C.c_int, [_P, _P]),
     "galaxy_bh_batch_footprint": (C.c_int, [_P, C.POINTER(BhConfig), _U32,
                                             C.POINTER(C.c_uint64)]),

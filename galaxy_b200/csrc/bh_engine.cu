@@ -1075,6 +1075,16 @@ extern "C" int galaxy_bh_read_tree_evidence(bh_device* dev, bh_tree* tree, TreeM
     return BH_OK;
 }
 
+extern "C" int galaxy_bh_tree_footprint(uint32_t n, const bh_config* cfg, uint64_t* bytes) {
+    if (!cfg || !bytes) return set_error(BH_INVALID_ARG, "null argument");
+    int rc = validate_config(cfg);
+    if (rc) return rc;
+    const uint32_t counts[1] = {n};
+    Layout L = plan_layout(counts, cfg, 1);
+    *bytes = plan_arena(L, 1).total();
+    return BH_OK;
+}
+
 extern "C" int galaxy_bh_tree_buffer_bytes(bh_tree* tree, uint64_t* bytes) {
     if (!tree || !bytes) return set_error(BH_INVALID_ARG, "null argument");
     *bytes = tree->batch->arena_bytes;

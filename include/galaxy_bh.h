@@ -194,6 +194,10 @@ int galaxy_bh_read_tree_evidence(bh_device* dev, bh_tree* tree, TreeMeta* meta,
                                  uint32_t cell_capacity, uint32_t* cell_count);
 /* ParallelTreeRuntime::buffer_bytes (nbody_parallel.rs:990-992). */
 int galaxy_bh_tree_buffer_bytes(bh_tree* tree, uint64_t* bytes);
+/* Device bytes galaxy_bh_tree_buffer_bytes reports for a tree of n bodies
+ * under cfg, without a device: the tree-buffer formula a receipt validator
+ * checks (the engine's counterpart of bench-bh2d-hardware.py:837-853). */
+int galaxy_bh_tree_footprint(uint32_t n, const bh_config* cfg, uint64_t* bytes);
 
 /* ---- BH #2B1 host-tree path -----------------------------------------------
  * NbodyGpu::traverse (nbody_gpu.rs:640-780) over a packed flat tree

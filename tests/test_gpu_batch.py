@@ -119,3 +119,15 @@ def test_autotune_batch_picks_admissible_settings(gpu):
     assert t.trials[-1][0] == "best" and t.trials[-1][2] > 0
     # tuning ran on copies: the caller's states are untouched
     assert before == [gpu.read_evolving_state_records(e)[0].tobytes() for e in evs]
+
+
+def test_receipt_run_passes_the_sweep_checks(gpu):
+    """A receipt of the reference sweep's workload (disc preset, 8192 bodies,
+    3 steps) produced on this engine passes the restated sweep validator."""
+    from galaxy_b200 import receipt
+    work = dict(particles=8192, preset="disc", steps=3, dt_myr=0.01, seed=303, theta=0.5,
+                softening_kpc=0.05, direct_probes=12, oracle_limit=4096, benchmark_warmup=2,
+                benchmark_repeats=7)
+    r = receipt.run_receipt(**work)
+    out = receipt.validate_receipt(r, **work)
+    assert out["leaf_count"] > 0 and r["tree"]["repeat_rebuild_matches"]
