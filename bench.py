@@ -230,7 +230,7 @@ def cpu_baseline_sample() -> dict:
 def run_engine(args, world, rank, local, pg):
     import torch
 
-    from galaxy_b200 import _lib
+    from galaxy_b200 import _lib, shard
     from galaxy_b200.nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime
 
     torch.cuda.set_device(local)
@@ -260,11 +260,8 @@ def run_engine(args, world, rank, local, pg):
         e1.record(stream)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
-    ms = e0.elapsed_time(e1)
+    ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")  # the slowest replica
     if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
         pg.barrier()
     value = world * N_BODIES * args.steps / (ms * 1e-3)
 
@@ -344,26 +341,19 @@ def run_engine(args, world, rank, local, pg):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_wall = time.perf_counter() - t0
-    e2e_ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
     e2e_value = world * N_BODIES * e2e_steps / (e2e_ms * 1e-3)
 
     tree.close()
     ev.close()
     batched = None
     if not args.no_batched:
-        batched = run_batched_leg(gpu, steps=min(args.steps, 20), warmup=args.warmup)
-        if pg:
-            t = torch.tensor([batched["ms_per_step"]], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            batched["value"] = world * batched["bodies"] / (float(t.item()) * 1e-3)
+        batched = run_batched_leg(gpu, steps=min(args.steps, 20), warmup=args.warmup, pg=pg,
+                                  rank=rank, world=world)
     served = None
     if not args.no_served:
-        served = run_served_leg(gpu, capacity=(batched or {}).get("value", value / world)
-                                / max(world, 1))
+        served = run_served_leg(gpu, capacity=(batched or {}).get("value", value), pg=pg,
+                                rank=rank, world=world)
     precision = None
     if not args.no_precision:
         precision = run_precision_leg(gpu, steps=args.precision_steps)
@@ -495,24 +485,28 @@ def run_precision_leg(gpu, steps: int = 500, n: int = 1 << 22, every: int = 10,
 
 
 def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps: int = 5,
-                    plain_sims: int | None = None) -> dict:
+                    plain_sims: int | None = None, pg=None, rank: int = 0, world: int = 1) -> dict:
     """Mixed workload: `count` independent simulations, N log-uniform in
     [2^10, 2^18], scenarios uniform over the three, per-simulation seeds,
     eps 0.01, theta 0.5, dt 1e-3.  Batched: one launch per stage for all of
     them.  Plain: each simulation alone through the plain path, one after
-    another (the same engine, tree per simulation)."""
+    another (the same engine, tree per simulation).  With several ranks the
+    simulations are placed by estimated work (galaxy_b200.shard), each rank
+    runs its share, and the rates use the slowest rank's time."""
     import torch
 
-    from galaxy_b200 import autotune, scenarios
+    from galaxy_b200 import autotune, scenarios, shard
     from galaxy_b200.batch import Batch
     from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
-    plan = scenarios.mixed_batch(count, 10, 18, seed=2024)
+    full_plan = scenarios.mixed_batch(count, 10, 18, seed=2024)
+    shares = shard.plan_shards([n for _, n, _ in full_plan], world)
+    plan = [full_plan[i] for i in shares[rank]]
     cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
     states = []
     for name, n, seed in plan:
         states.append(gpu.create_evolving_state_records(
             bodies_to_state(scenarios.make(name, n, seed, eps=0.01)))[0])
-    total = sum(s.count for s in states)
+    total = int(shard.sum_over_ranks(pg, sum(s.count for s in states)))
     stream = torch.cuda.ExternalStream(gpu.stream_ptr())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -532,7 +526,7 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
         batch.step(1e-3, steps)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
         arena = batch.arena_bytes()
         batch.close()
         return ms, arena
@@ -560,8 +554,8 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
         rt.step(gpu, s, t, cfg, 1e-3, plain_steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    p_ms = e0.elapsed_time(e1)
-    p_bodies = sum(s.count for s in sims)
+    p_ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
+    p_bodies = shard.sum_over_ranks(pg, sum(s.count for s in sims))
     for t in trees:
         t.close()
     for s in states:
@@ -576,13 +570,14 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
             "tuning": tuning.as_dict(), "tuning_force_error_median": tuning.errors,
             "untuned": {"value": total * steps / (u_ms * 1e-3), "ms_per_step": u_ms / steps,
                         "settings": "leaf size 1, 8-bit digits, 4 traversal warps (defaults)"},
-            "plain_serial": {"value": plain, "steps": plain_steps, "sims": len(sims),
+            "ranks": world,
+            "plain_serial": {"value": plain, "steps": plain_steps, "sims": len(sims) * world,
                              "ms_per_step": p_ms / plain_steps},
             "speedup_vs_plain": batched / plain}
 
 
 def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: float = 150.0,
-                   deadline: float = 120.0) -> dict:
+                   deadline: float = 120.0, pg=None, rank: int = 0, world: int = 1) -> dict:
     """Served workload: Poisson arrivals, N log-uniform [2^12, 2^22], steps
     log-uniform [10, 1000], scenario uniform, theta 0.5, eps 0.01, dt 1e-3,
     admitted against a 150 GB budget and continuously batched; each request
@@ -594,10 +589,14 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
     Throughput: the specified 200/s stream for 0.2 s (a saturating burst of
     ~40 requests) served with continuous batching, against the same requests
     run one after another through the plain path (both include state upload,
-    tree allocation, boundary solve and all steps)."""
+    tree allocation, boundary solve and all steps).  With several ranks
+    (`capacity` is then the whole job's) every rank draws the same request
+    stream and serves the requests placed on it by estimated work
+    (galaxy_b200.shard); latencies are pooled over ranks and rates use the
+    slowest rank's wall time."""
     import torch
 
-    from galaxy_b200 import scenarios
+    from galaxy_b200 import scenarios, shard
     from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
     from galaxy_b200.serve import GpuEngineOps, Server, poisson_requests
     mean_work = 605_000 * 215.0  # E[N] * E[steps] of the distributions above
@@ -613,14 +612,31 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
         return reqs
 
     budget = int(budget_gb * 2 ** 30)
-    reqs = with_inputs(poisson_requests(rate, duration, seed=11))
-    out = Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16).run(reqs,
-                                                                           deadline=deadline)
+
+    def my_share(reqs):
+        shares = shard.plan_shards([r.n for r in reqs], world, steps=[r.steps for r in reqs])
+        return [reqs[i] for i in shares[rank]]
+
+    def pooled(out, mine):
+        if world == 1:
+            return out
+        lat = [x for part in shard.gather_to_all(pg, [r.latency for r in mine
+                                                       if r.latency is not None]) for x in part]
+        wall = shard.max_over_ranks(pg, out["wall_s"])
+        steps_done = shard.sum_over_ranks(pg, out["particle_steps"])
+        return dict(out, requests=int(shard.sum_over_ranks(pg, out["requests"])),
+                    completed=len(lat), p50_s=float(np.percentile(lat, 50)) if lat else None,
+                    p99_s=float(np.percentile(lat, 99)) if lat else None, wall_s=wall,
+                    particle_steps=steps_done, particle_steps_per_s=steps_done / wall)
+
+    reqs = with_inputs(my_share(poisson_requests(rate, duration, seed=11)))
+    out = pooled(Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16)
+                 .run(reqs, deadline=deadline), reqs)
     for r in reqs:
         r.bodies = None
-    burst = with_inputs(poisson_requests(200.0, 0.2, seed=12))
-    sat = Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16).run(burst,
-                                                                           deadline=deadline)
+    burst = with_inputs(my_share(poisson_requests(200.0, 0.2, seed=12)))
+    sat = pooled(Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16)
+                 .run(burst, deadline=deadline), burst)
     torch.cuda.synchronize()
     rt = ParallelTreeRuntime(gpu)
     t0 = time.perf_counter()
@@ -634,7 +650,7 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
         tree.close()
         ev.close()
         ps += r.n * r.steps
-    plain = ps / (time.perf_counter() - t0)
+    plain = shard.sum_over_ranks(pg, ps) / shard.max_over_ranks(pg, time.perf_counter() - t0)
     return {
         "workload": "Poisson arrivals, N log-uniform [2^12,2^22], steps log-uniform [10,1000], "
                     "mixed scenarios, theta 0.5, eps 0.01, dt 1e-3, 150 GB budget",
@@ -642,7 +658,8 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
         "specified_rate_per_s": 200.0,
         "specified_load_factor": 200.0 * mean_work / capacity,
         "saturated": dict(sat, rate_per_s=200.0, arrival_window_s=0.2),
-        "plain_serial": {"particle_steps_per_s": plain, "requests": len(burst),
+        "ranks": world,
+        "plain_serial": {"particle_steps_per_s": plain, "requests": sat["requests"],
                          "includes": "state upload, tree allocation, boundary solve, steps"},
         "speedup_vs_plain": sat["particle_steps_per_s"] / plain if plain else None}
 
