@@ -420,3 +420,39 @@ def test_force_after_step_reproduces_step_accelerations(gpu, rt):
     assert np.array_equal(a_step.view(np.uint32), a_plain.view(np.uint32))
     c = gpu.conservation(ev)
     assert c["potential"] < 0.0 and np.isfinite(c["energy"])
+
+
+@pytest.mark.parametrize("case", ["two", "three", "coincident", "self_exclusion", "line"])
+def test_forces_on_small_and_degenerate_systems(gpu, rt, oracle, case):
+    """The smallest systems, bodies sharing one position (a chain to depth
+    16), a body next to another inside one cell at theta 2 (self exclusion
+    by the Morton range, flat.rs:539-564) and collinear bodies: bit-exact
+    tree, the reference's decisions, forces within tolerance."""
+    theta = 0.5
+    if case == "two":
+        rows = [[0.0, 0.0, 1.0], [1.0, 0.0, 2.0]]
+    elif case == "three":
+        rows = [[0.0, 0.0, 1.0], [1.0, 0.0, 1.0], [0.0, 1.0, 1.0]]
+    elif case == "coincident":
+        rows = [[0.25, -0.5, 1.0]] * 8 + [[1.0, 1.0, 1.0], [-1.0, 0.5, 3.0]]
+    elif case == "self_exclusion":
+        theta = 2.0
+        rows = [[0.0, 0.0, 1.0], [1e-3, 0.0, 1.0], [5.0, 5.0, 1.0], [-4.0, 3.0, 2.0]]
+    else:
+        rows = [[x, 0.0, 1.0 + 0.1 * i] for i, x in enumerate(np.linspace(-1, 1, 37))]
+    bodies = np.zeros((len(rows), 5))
+    bodies[:, [0, 1, 4]] = np.array(rows)
+    cfg = Config(theta=theta, softening_kpc=0.1 if case == "coincident" else 0.01, g=1.0,
+                 bucket=1)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    assert np.isfinite(acc).all()
+    rel, stats = force_check(oracle, acc, b32, ot, oc)
+    gs = rt.force_stats(gpu, tree)
+    assert gs["visited_nodes"] == stats["visited_nodes"]
+    assert gs["approximated_cells"] == stats["approximated_cells"]
+    assert gs["direct_terms"] == stats["direct_terms"]
+    rt.step(gpu, ev, tree, cfg, 1e-3, 3)
+    assert np.isfinite(gpu.read_evolving_state(ev)[0]).all()
