@@ -83,6 +83,23 @@ class BhTuning(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
 
+class BhServeConfig(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("round_steps", C.c_uint32),
+                ("max_members", C.c_uint32)]
+
+
+class BhServeResult(C.Structure):
+    _fields_ = [("request_id", C.c_uint64), ("n", C.c_uint32), ("status", C.c_uint32),
+                ("steps", C.c_uint32), ("reserved", C.c_uint32), ("submitted_s", C.c_double),
+                ("admitted_s", C.c_double), ("finished_s", C.c_double)]
+
+
+class BhServeStats(C.Structure):
+    _fields_ = [("rounds", C.c_uint64), ("particle_steps", C.c_uint64),
+                ("completed", C.c_uint64), ("busy_seconds", C.c_double),
+                ("elapsed_seconds", C.c_double)]
+
+
 class BhForceStats(C.Structure):
     _fields_ = [("visited_nodes", C.c_uint64), ("approximated_cells", C.c_uint64),
                 ("direct_terms", C.c_uint64), ("exact_mac_fallbacks", C.c_uint64),
@@ -131,6 +148,12 @@ SIGNATURES = {
     "galaxy_bh_batch_step": (C.c_int, [_P, _P, C.POINTER(C.c_double), _U32]),
     "galaxy_bh_batch_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "galaxy_bh_batch_tune": (C.c_int, [_P, _P]),
+    "galaxy_bh_serve_start": (C.c_int, [C.c_int, _P, C.POINTER(C.c_void_p)]),
+    "galaxy_bh_serve_submit": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_double, C.c_uint32,
+                                         C.POINTER(C.c_uint64)]),
+    "galaxy_bh_serve_poll": (C.c_int, [_P, C.c_uint32, _P, _P, C.c_uint32]),
+    "galaxy_bh_serve_stats": (C.c_int, [_P, _P]),
+    "galaxy_bh_serve_stop": (C.c_int, [_P]),
     "galaxy_bh_tree_footprint": (C.c_int, [C.c_uint32, _P, C.POINTER(C.c_uint64)]),
     "galaxy_bh_tree_tune": (C.c_int, [_P, _P]),
     "galaxy_bh_batch_footprint": (C.c_int, [_P, C.POINTER(BhConfig), _U32,

@@ -5,7 +5,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgalaxy_bh.so")
-SOURCES = ["bh_kernels.cu", "bh_engine.cu", "bh_noalloc.cu"]
+SOURCES = ["bh_kernels.cu", "bh_engine.cu", "bh_noalloc.cu", "bh_serve.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -1,0 +1,297 @@
+// SPDX-License-Identifier: Apache-2.0
+// Native continuous-batching server over the public C ABI (galaxy_bh.h).
+//
+// One host thread owns a device handle and runs the serving loop: submitted
+// requests (initial state records, config, dt, step count) wait in arrival
+// order and are admitted as soon as the device-memory footprint of the
+// active set plus the newcomer fits the budget; admitted simulations stay
+// resident and advance together, a round of fused KDK steps at a time, in one
+// batch (one launch per stage for all of them).  A round stops at the
+// smallest remaining step count, so finished simulations leave and waiting
+// ones join between rounds.  Finished results are copied back and queued for
+// galaxy_bh_serve_poll.  Each simulation's result equals its result alone:
+// batch members never interact.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "bh_internal.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServeRequest {
+    uint64_t id = 0;
+    std::vector<GpuEvolveState> records;  // initial state, then the result
+    bh_config cfg{};
+    double dt = 0.0;
+    uint32_t n = 0, steps = 0, remaining = 0;
+    int status = BH_OK;
+    double submitted_s = 0.0, admitted_s = -1.0, finished_s = -1.0;
+    bh_state* st = nullptr;
+};
+
+}  // namespace
+
+struct bh_server {
+    bh_device* dev = nullptr;
+    bh_serve_config sc{};
+    Clock::time_point t0;
+    std::thread loop;
+    std::mutex mu;
+    std::condition_variable cv_in, cv_out;
+    std::deque<std::unique_ptr<ServeRequest>> submitted, done;
+    bool stopping = false;
+    uint64_t next_id = 1;
+    uint64_t rounds = 0, particle_steps = 0, completed = 0;
+    double busy_s = 0.0;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+void finish(bh_server* s, std::unique_ptr<ServeRequest> r) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (r->status == BH_OK) ++s->completed;
+    s->done.push_back(std::move(r));
+    s->cv_out.notify_all();
+}
+
+void release_state(std::unique_ptr<ServeRequest>& r) {
+    if (r->st) galaxy_bh_state_destroy(r->st);
+    r->st = nullptr;
+}
+
+int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active, bh_batch** b) {
+    if (*b) galaxy_bh_batch_destroy(*b);
+    *b = nullptr;
+    if (active.empty()) return BH_OK;
+    std::vector<bh_state*> states;
+    std::vector<bh_config> cfgs;
+    for (auto& r : active) {
+        states.push_back(r->st);
+        cfgs.push_back(r->cfg);
+    }
+    return galaxy_bh_batch_create(s->dev, states.data(), cfgs.data(), (uint32_t)states.size(), b);
+}
+
+void serve_loop(bh_server* s) {
+    std::deque<std::unique_ptr<ServeRequest>> waiting;
+    std::vector<std::unique_ptr<ServeRequest>> active;
+    bh_batch* batch = nullptr;
+    auto fail_all_active = [&](int rc) {
+        for (auto& r : active) {
+            release_state(r);
+            r->status = rc;
+            r->finished_s = s->now();
+            finish(s, std::move(r));
+        }
+        active.clear();
+        if (batch) galaxy_bh_batch_destroy(batch);
+        batch = nullptr;
+    };
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (s->stopping) break;
+            while (!s->submitted.empty()) {
+                waiting.push_back(std::move(s->submitted.front()));
+                s->submitted.pop_front();
+            }
+            if (waiting.empty() && active.empty()) {
+                s->cv_in.wait_for(lk, std::chrono::milliseconds(50));
+                continue;
+            }
+        }
+        // admission, in arrival order, against the device-memory budget
+        bool joined = false;
+        while (!waiting.empty() && active.size() < s->sc.max_members) {
+            std::unique_ptr<ServeRequest>& cand = waiting.front();
+            std::vector<uint32_t> counts;
+            std::vector<bh_config> cfgs;
+            for (auto& r : active) {
+                counts.push_back(r->n);
+                cfgs.push_back(r->cfg);
+            }
+            counts.push_back(cand->n);
+            cfgs.push_back(cand->cfg);
+            uint64_t bytes = 0;
+            int rc = galaxy_bh_batch_footprint(counts.data(), cfgs.data(),
+                                               (uint32_t)counts.size(), &bytes);
+            if (rc == BH_OK && bytes > s->sc.budget_bytes) {
+                if (!active.empty()) break;  // wait for room
+                rc = BH_CAPACITY_OVERFLOW;   // alone it can never fit
+            }
+            if (rc == BH_OK)
+                rc = galaxy_bh_state_create(s->dev, cand->records.data(), cand->n, &cand->st,
+                                            nullptr);
+            std::unique_ptr<ServeRequest> r = std::move(cand);
+            waiting.pop_front();
+            if (rc != BH_OK) {
+                r->status = rc;
+                r->finished_s = s->now();
+                finish(s, std::move(r));
+                continue;
+            }
+            r->admitted_s = s->now();
+            r->remaining = r->steps;
+            active.push_back(std::move(r));
+            joined = true;
+        }
+        if (active.empty()) continue;
+        if (joined) {
+            // new members need their boundary acceleration; for members already
+            // stepping the solve reproduces theirs (same positions and tree)
+            int rc = form_batch(s, active, &batch);
+            if (rc == BH_OK) rc = galaxy_bh_batch_solve(s->dev, batch);
+            if (rc != BH_OK) {
+                fail_all_active(rc);
+                continue;
+            }
+        }
+        uint32_t r_steps = s->sc.round_steps;
+        uint64_t bodies = 0;
+        std::vector<double> dts;
+        for (auto& r : active) {
+            r_steps = std::min(r_steps, r->remaining);
+            bodies += r->n;
+            dts.push_back(r->dt);
+        }
+        const double tb = s->now();
+        int rc = galaxy_bh_batch_step(s->dev, batch, dts.data(), r_steps);
+        if (rc != BH_OK) {
+            fail_all_active(rc);
+            continue;
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->busy_s += s->now() - tb;
+            ++s->rounds;
+            s->particle_steps += bodies * r_steps;
+        }
+        std::vector<std::unique_ptr<ServeRequest>> still;
+        bool left = false;
+        for (auto& r : active) {
+            r->remaining -= r_steps;
+            if (r->remaining == 0) {
+                r->status = galaxy_bh_read_state(s->dev, r->st, r->records.data(), r->n, nullptr);
+                r->finished_s = s->now();
+                release_state(r);
+                finish(s, std::move(r));
+                left = true;
+            } else {
+                still.push_back(std::move(r));
+            }
+        }
+        active = std::move(still);
+        if (left) {
+            // re-formed batches step at once: every member's acceleration
+            // buffer holds its boundary acceleration
+            if ((rc = form_batch(s, active, &batch)) != BH_OK) fail_all_active(rc);
+        }
+    }
+    if (batch) galaxy_bh_batch_destroy(batch);
+    for (auto& r : active) release_state(r);
+}
+
+}  // namespace
+
+using gbh::set_error_message;
+
+extern "C" int galaxy_bh_serve_start(int ordinal, const bh_serve_config* config,
+                                     bh_server** out) {
+    if (!config || !out) return set_error_message(BH_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (config->round_steps == 0 || config->max_members == 0 || config->budget_bytes == 0)
+        return set_error_message(BH_INVALID_ARG,
+                                 "serve config needs a budget, round_steps and max_members");
+    bh_device* dev = nullptr;
+    int rc = galaxy_bh_device_open(ordinal, &dev);
+    if (rc != BH_OK) return rc;
+    bh_server* s = new bh_server();
+    s->dev = dev;
+    s->sc = *config;
+    s->t0 = Clock::now();
+    s->loop = std::thread(serve_loop, s);
+    *out = s;
+    return BH_OK;
+}
+
+extern "C" int galaxy_bh_serve_submit(bh_server* s, const GpuEvolveState* host, uint32_t n,
+                                      const bh_config* cfg, double dt, uint32_t steps,
+                                      uint64_t* request_id) {
+    if (!s || !host || !cfg || !request_id)
+        return set_error_message(BH_INVALID_ARG, "null argument");
+    if (n < 2 || steps == 0)
+        return set_error_message(BH_INVALID_ARG, "a request needs n >= 2 bodies and steps >= 1");
+    auto r = std::make_unique<ServeRequest>();
+    r->records.assign(host, host + n);
+    r->cfg = *cfg;
+    r->dt = dt;
+    r->n = n;
+    r->steps = steps;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) return set_error_message(BH_INVALID_ARG, "server is stopping");
+    r->id = s->next_id++;
+    r->submitted_s = s->now();
+    *request_id = r->id;
+    s->submitted.push_back(std::move(r));
+    s->cv_in.notify_all();
+    return BH_OK;
+}
+
+extern "C" int galaxy_bh_serve_poll(bh_server* s, uint32_t timeout_ms, bh_serve_result* res,
+                                    GpuEvolveState* out, uint32_t capacity) {
+    if (!s || !res) return set_error_message(BH_INVALID_ARG, "null argument");
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (!s->cv_out.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                            [&] { return !s->done.empty(); }))
+        return set_error_message(BH_TIMEOUT, "no finished request within the timeout");
+    ServeRequest& r = *s->done.front();
+    if (r.status == BH_OK && (!out || capacity < r.n))
+        return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
+    res->request_id = r.id;
+    res->n = r.n;
+    res->status = (uint32_t)r.status;
+    res->steps = r.steps;
+    res->submitted_s = r.submitted_s;
+    res->admitted_s = r.admitted_s;
+    res->finished_s = r.finished_s;
+    if (r.status == BH_OK) std::memcpy(out, r.records.data(), sizeof(GpuEvolveState) * r.n);
+    s->done.pop_front();
+    return BH_OK;
+}
+
+extern "C" int galaxy_bh_serve_stats(bh_server* s, bh_serve_stats* out) {
+    if (!s || !out) return set_error_message(BH_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->rounds = s->rounds;
+    out->particle_steps = s->particle_steps;
+    out->completed = s->completed;
+    out->busy_seconds = s->busy_s;
+    out->elapsed_seconds = s->now();
+    return BH_OK;
+}
+
+extern "C" int galaxy_bh_serve_stop(bh_server* s) {
+    if (!s) return BH_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        s->cv_in.notify_all();
+    }
+    if (s->loop.joinable()) s->loop.join();
+    galaxy_bh_device_close(s->dev);
+    delete s;
+    return BH_OK;
+}

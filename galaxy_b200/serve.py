@@ -217,3 +217,62 @@ class GpuEngineOps(EngineOps):
 
     def release_batch(self, batch):
         batch.close()
+
+
+class NativeServer:
+    """The serving loop of the C ABI (galaxy_bh_serve_*): its own host
+    thread and device handle; submit from here, poll for results."""
+
+    def __init__(self, ordinal: int = 0, budget_bytes: int = 150 << 30, round_steps: int = 16,
+                 max_members: int = 4096):
+        import ctypes as C
+
+        from . import _lib
+        self._C, self._lib = C, _lib
+        cfg = _lib.BhServeConfig(int(budget_bytes), int(round_steps), int(max_members))
+        self._h = C.c_void_p()
+        _lib.check(_lib.load().galaxy_bh_serve_start(int(ordinal), C.byref(cfg),
+                                                     C.byref(self._h)))
+        self._n: dict[int, int] = {}
+
+    def submit(self, records: np.ndarray, config, dt: float, steps: int) -> int:
+        """Queues a simulation (GpuEvolveState records); returns its id."""
+        C, _lib = self._C, self._lib
+        rec = np.ascontiguousarray(records, dtype=_lib.EVOLVE_STATE_DTYPE)
+        rid = C.c_uint64()
+        _lib.check(_lib.load().galaxy_bh_serve_submit(self._h, _lib.ptr(rec), len(rec),
+                                                      C.byref(config.to_c()), float(dt),
+                                                      int(steps), C.byref(rid)))
+        self._n[rid.value] = len(rec)
+        return rid.value
+
+    def poll(self, timeout_s: float = 0.0):
+        """(result info dict, final records) of the next finished request, or
+        None when none finishes within the timeout."""
+        C, _lib = self._C, self._lib
+        res = _lib.BhServeResult()
+        cap = max(self._n.values()) if self._n else 0
+        out = np.zeros(cap, _lib.EVOLVE_STATE_DTYPE)
+        rc = _lib.load().galaxy_bh_serve_poll(self._h, int(timeout_s * 1000), C.byref(res),
+                                              _lib.ptr(out), cap)
+        if rc == _lib.BH_TIMEOUT:
+            return None
+        _lib.check(rc)
+        self._n.pop(res.request_id, None)
+        info = {"request_id": res.request_id, "n": res.n, "status": res.status,
+                "steps": res.steps, "submitted_s": res.submitted_s,
+                "admitted_s": res.admitted_s, "finished_s": res.finished_s}
+        return info, (out[:res.n].copy() if res.status == _lib.BH_OK else None)
+
+    def stats(self) -> dict:
+        C, _lib = self._C, self._lib
+        st = _lib.BhServeStats()
+        _lib.check(_lib.load().galaxy_bh_serve_stats(self._h, C.byref(st)))
+        return {"rounds": st.rounds, "particle_steps": st.particle_steps,
+                "completed": st.completed, "busy_seconds": st.busy_seconds,
+                "elapsed_seconds": st.elapsed_seconds}
+
+    def stop(self) -> None:
+        if self._h:
+            self._lib.load().galaxy_bh_serve_stop(self._h)
+            self._h = self._C.c_void_p()

@@ -272,6 +272,48 @@ int galaxy_bh_batch_solve(bh_device* dev, bh_batch* batch);
 int galaxy_bh_batch_step(bh_device* dev, bh_batch* batch, const double* dts, uint32_t nsteps);
 int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
 
+/* ---- native serving loop --------------------------------------------------
+ * No reference counterpart (the reference has no serving path).  A server
+ * owns a device handle and one host thread running continuous batching:
+ * submitted simulations wait in arrival order, are admitted when the
+ * device-memory footprint of the active set plus the newcomer (the
+ * galaxy_bh_batch_footprint figure) fits budget_bytes, stay resident, and
+ * advance together in rounds of at most round_steps fused KDK steps in one
+ * batch; a round stops at the smallest remaining step count so finished
+ * simulations leave and waiting ones join between rounds.  Each result
+ * equals the same simulation stepped alone.  submit copies the initial
+ * records; poll waits up to timeout_ms for a finished request (BH_TIMEOUT if
+ * none), fills *result (status = the request's bh_status: a request that can
+ * never fit the budget fails with BH_CAPACITY_OVERFLOW) and copies its final
+ * records to out (capacity >= n).  submit, poll and stats may be called from
+ * any host thread; stop ends the loop after the current round, drops
+ * unfinished requests and frees everything. */
+typedef struct bh_server bh_server;
+typedef struct {
+    uint64_t budget_bytes;
+    uint32_t round_steps;
+    uint32_t max_members;
+} bh_serve_config;
+typedef struct {
+    uint64_t request_id;
+    uint32_t n;
+    uint32_t status;
+    uint32_t steps;
+    uint32_t reserved;
+    double submitted_s, admitted_s, finished_s;  /* seconds since serve_start */
+} bh_serve_result;
+typedef struct {
+    uint64_t rounds, particle_steps, completed;
+    double busy_seconds, elapsed_seconds;
+} bh_serve_stats;
+int galaxy_bh_serve_start(int ordinal, const bh_serve_config* config, bh_server** out);
+int galaxy_bh_serve_submit(bh_server* server, const GpuEvolveState* host, uint32_t n,
+                           const bh_config* cfg, double dt, uint32_t steps, uint64_t* request_id);
+int galaxy_bh_serve_poll(bh_server* server, uint32_t timeout_ms, bh_serve_result* result,
+                         GpuEvolveState* out, uint32_t capacity);
+int galaxy_bh_serve_stats(bh_server* server, bh_serve_stats* out);
+int galaxy_bh_serve_stop(bh_server* server);
+
 /* ---- launch-shape tuning --------------------------------------------------
  * No reference counterpart (the reference's WGSL dispatch shapes are fixed).
  * Knobs the autotuner (galaxy_b200/autotune.py) picks per batch or tree;

@@ -144,3 +144,79 @@ def test_served_results_equal_alone():
         rt.step(gpu, ev, tree, cfg, r.dt, r.steps)
         alone = gpu.read_evolving_state_records(ev)[0]
         assert alone.tobytes() == r.result.tobytes(), f"request {r.rid}"
+
+
+def test_native_server_needs_a_device_and_a_config():
+    import ctypes as C
+
+    from galaxy_b200 import _lib, build
+    build.build()
+    lib = _lib.load()
+    h = C.c_void_p()
+    bad = _lib.BhServeConfig(0, 16, 8)
+    assert lib.galaxy_bh_serve_start(0, C.byref(bad), C.byref(h)) != _lib.BH_OK
+    if not _gpu_available():
+        good = _lib.BhServeConfig(1 << 30, 16, 8)
+        assert lib.galaxy_bh_serve_start(0, C.byref(good), C.byref(h)) == _lib.BH_NO_DEVICE
+
+
+def _gpu_available() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.gpu
+def test_native_server_results_equal_alone():
+    """Requests of uneven size, configs and step counts, submitted while others
+    run, finish bit-identical to the same simulations stepped alone; one that
+    can never fit the budget fails on its own."""
+    import time
+
+    from galaxy_b200 import _lib, scenarios
+    from galaxy_b200.batch import footprint_bytes
+    from galaxy_b200.nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime, bodies_to_state
+    from galaxy_b200.serve import NativeServer
+
+    plan = [("exponential_disc", 20000, 3, 23, Config(theta=0.5, softening_kpc=0.01, g=1.0)),
+            ("cold_disc", 5000, 4, 7, Config(theta=0.7, softening_kpc=0.01, g=1.0, bucket=4)),
+            ("binary_encounter", 12000, 5, 15, Config(theta=0.3, softening_kpc=0.005, g=1.0)),
+            ("cold_disc", 3000, 6, 40, Config(theta=0.5, softening_kpc=0.01, g=1.0,
+                                              compensated=True))]
+    budget = footprint_bytes([20000, 5000, 12000], [p[4] for p in plan[:3]])
+    srv = NativeServer(0, budget_bytes=budget, round_steps=4)
+    try:
+        ids = {}
+        for k, (name, n, seed, steps, cfg) in enumerate(plan):
+            rec = bodies_to_state(scenarios.make(name, n, seed, eps=0.01))
+            ids[srv.submit(rec, cfg, 1e-3, steps)] = k
+            time.sleep(0.01)
+        too_big = srv.submit(bodies_to_state(scenarios.make("cold_disc", 400000, 9)),
+                             plan[0][4], 1e-3, 2)
+        results, failed = {}, {}
+        while len(results) + len(failed) < len(plan) + 1:
+            got = srv.poll(timeout_s=30.0)
+            assert got is not None, "server stalled"
+            info, rec = got
+            if info["status"] == _lib.BH_OK:
+                results[ids[info["request_id"]]] = rec
+            else:
+                failed[info["request_id"]] = info["status"]
+        assert failed == {too_big: _lib.BH_CAPACITY_OVERFLOW}
+        st = srv.stats()
+        assert st["completed"] == len(plan) and st["rounds"] >= 10
+    finally:
+        srv.stop()
+    gpu = NbodyGpu("0")
+    rt = ParallelTreeRuntime(gpu)
+    for k, (name, n, seed, steps, cfg) in enumerate(plan):
+        ev, _ = gpu.create_evolving_state_records(bodies_to_state(scenarios.make(name, n, seed,
+                                                                                 eps=0.01)))
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        rt.step(gpu, ev, tree, cfg, 1e-3, steps)
+        alone, _ = gpu.read_evolving_state_records(ev)
+        assert np.array_equal(alone.view(np.uint32), results[k].view(np.uint32)), name
