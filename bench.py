@@ -598,7 +598,7 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
 
     from galaxy_b200 import scenarios, shard
     from galaxy_b200.nbody_gpu import Config, ParallelTreeRuntime, bodies_to_state
-    from galaxy_b200.serve import GpuEngineOps, Server, poisson_requests
+    from galaxy_b200.serve import NativeServer, poisson_requests
     mean_work = 605_000 * 215.0  # E[N] * E[steps] of the distributions above
     rate = max(0.2, 0.6 * capacity / mean_work)
     cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
@@ -629,14 +629,65 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
                     p99_s=float(np.percentile(lat, 99)) if lat else None, wall_s=wall,
                     particle_steps=steps_done, particle_steps_per_s=steps_done / wall)
 
+    def serve(reqs):
+        """The native server (galaxy_bh_serve_*): a submitter thread releases
+        each request at its arrival time, this thread polls for results;
+        latency = finish - arrival."""
+        import threading
+        srv = NativeServer(gpu.info()["index"], budget_bytes=budget, round_steps=16)
+        recs = [bodies_to_state(r.bodies) for r in reqs]
+        ids = {}
+        t0 = time.perf_counter()
+
+        def submitter():
+            for r, rec in zip(reqs, recs):
+                delay = r.arrival - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids[srv.submit(rec, cfg, r.dt, r.steps)] = r
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        done, ps, first_submit, last_finish = 0, 0, None, 0.0
+
+        def collect():
+            nonlocal done, ps, first_submit, last_finish
+            while done < len(reqs) and time.perf_counter() - t0 < deadline:
+                got = srv.poll(timeout_s=1.0)
+                if got is None:
+                    continue
+                info, _ = got
+                done += 1
+                while info["request_id"] not in ids:  # the submitter records ids after submit
+                    time.sleep(1e-4)
+                r = ids[info["request_id"]]
+                r.finished = r.arrival + (info["finished_s"] - info["submitted_s"])
+                ps += r.n * r.steps
+                first_submit = info["submitted_s"] if first_submit is None else \
+                    min(first_submit, info["submitted_s"])
+                last_finish = max(last_finish, info["finished_s"])
+
+        try:
+            collect()
+        finally:
+            th.join()
+            st = srv.stats()
+            srv.stop()
+        wall = (last_finish - first_submit) if first_submit is not None else 0.0
+        lat = np.array([r.latency for r in reqs if r.latency is not None])
+        return {"requests": len(reqs), "completed": int(len(lat)),
+                "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+                "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+                "wall_s": wall, "busy_s": st["busy_seconds"], "rounds": st["rounds"],
+                "particle_steps": ps, "particle_steps_per_s": ps / wall if wall > 0 else 0.0,
+                "server": "native (galaxy_bh_serve_*)"}
+
     reqs = with_inputs(my_share(poisson_requests(rate, duration, seed=11)))
-    out = pooled(Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16)
-                 .run(reqs, deadline=deadline), reqs)
+    out = pooled(serve(reqs), reqs)
     for r in reqs:
         r.bodies = None
     burst = with_inputs(my_share(poisson_requests(200.0, 0.2, seed=12)))
-    sat = pooled(Server(GpuEngineOps(gpu, cfg, bodies), budget, round_steps=16)
-                 .run(burst, deadline=deadline), burst)
+    sat = pooled(serve(burst), burst)
     torch.cuda.synchronize()
     rt = ParallelTreeRuntime(gpu)
     t0 = time.perf_counter()

@@ -258,9 +258,10 @@ extern "C" int galaxy_bh_serve_poll(bh_server* s, uint32_t timeout_ms, bh_serve_
                             [&] { return !s->done.empty(); }))
         return set_error_message(BH_TIMEOUT, "no finished request within the timeout");
     ServeRequest& r = *s->done.front();
-    if (r.status == BH_OK && (!out || capacity < r.n))
-        return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
     res->request_id = r.id;
+    res->n = r.n;
+    if (r.status == BH_OK && (!out || capacity < r.n))  // kept for a retry with room
+        return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
     res->n = r.n;
     res->status = (uint32_t)r.status;
     res->steps = r.steps;

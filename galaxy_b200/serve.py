@@ -16,6 +16,7 @@ be exercised without a GPU.
 """
 from __future__ import annotations
 
+import atexit
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -233,17 +234,18 @@ class NativeServer:
         self._h = C.c_void_p()
         _lib.check(_lib.load().galaxy_bh_serve_start(int(ordinal), C.byref(cfg),
                                                      C.byref(self._h)))
-        self._n: dict[int, int] = {}
+        self._max_n = 0
+        _LIVE_SERVERS.add(self)
 
     def submit(self, records: np.ndarray, config, dt: float, steps: int) -> int:
         """Queues a simulation (GpuEvolveState records); returns its id."""
         C, _lib = self._C, self._lib
         rec = np.ascontiguousarray(records, dtype=_lib.EVOLVE_STATE_DTYPE)
+        self._max_n = max(self._max_n, len(rec))  # before the server can finish it
         rid = C.c_uint64()
         _lib.check(_lib.load().galaxy_bh_serve_submit(self._h, _lib.ptr(rec), len(rec),
                                                       C.byref(config.to_c()), float(dt),
                                                       int(steps), C.byref(rid)))
-        self._n[rid.value] = len(rec)
         return rid.value
 
     def poll(self, timeout_s: float = 0.0):
@@ -251,14 +253,17 @@ class NativeServer:
         None when none finishes within the timeout."""
         C, _lib = self._C, self._lib
         res = _lib.BhServeResult()
-        cap = max(self._n.values()) if self._n else 0
-        out = np.zeros(cap, _lib.EVOLVE_STATE_DTYPE)
+        cap = self._max_n
+        out = np.zeros(max(cap, 1), _lib.EVOLVE_STATE_DTYPE)
         rc = _lib.load().galaxy_bh_serve_poll(self._h, int(timeout_s * 1000), C.byref(res),
                                               _lib.ptr(out), cap)
         if rc == _lib.BH_TIMEOUT:
             return None
+        if rc == _lib.BH_INVALID_ARG and res.n > cap:  # sized by another submitter
+            cap = res.n
+            out = np.zeros(cap, _lib.EVOLVE_STATE_DTYPE)
+            rc = _lib.load().galaxy_bh_serve_poll(self._h, 0, C.byref(res), _lib.ptr(out), cap)
         _lib.check(rc)
-        self._n.pop(res.request_id, None)
         info = {"request_id": res.request_id, "n": res.n, "status": res.status,
                 "steps": res.steps, "submitted_s": res.submitted_s,
                 "admitted_s": res.admitted_s, "finished_s": res.finished_s}
@@ -273,6 +278,32 @@ class NativeServer:
                 "elapsed_seconds": st.elapsed_seconds}
 
     def stop(self) -> None:
+        """Ends the loop and joins its thread; always call it (or use the
+        server as a context manager) before the process exits."""
         if self._h:
             self._lib.load().galaxy_bh_serve_stop(self._h)
             self._h = self._C.c_void_p()
+        _LIVE_SERVERS.discard(self)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
+_LIVE_SERVERS: set = set()
+
+
+def _stop_live_servers():
+    for srv in list(_LIVE_SERVERS):
+        srv.stop()
+
+
+atexit.register(_stop_live_servers)

@@ -285,7 +285,9 @@ int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
  * records; poll waits up to timeout_ms for a finished request (BH_TIMEOUT if
  * none), fills *result (status = the request's bh_status: a request that can
  * never fit the budget fails with BH_CAPACITY_OVERFLOW) and copies its final
- * records to out (capacity >= n).  submit, poll and stats may be called from
+ * records to out (capacity >= n; with less room it returns BH_INVALID_ARG,
+ * sets result->request_id and result->n and keeps the result queued).
+ * submit, poll and stats may be called from
  * any host thread; stop ends the loop after the current round, drops
  * unfinished requests and frees everything. */
 typedef struct bh_server bh_server;
