@@ -35,9 +35,41 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+#ifndef GBH_PDL
+#define GBH_PDL 1
+#endif
+
+// Launches a kernel of the step with programmatic stream serialization, so
+// its launch overlaps the previous kernel's tail (see wait_for_predecessor).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_step(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                               cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = GBH_PDL;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ void set_err(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
+
+// Programmatic dependent launch: a kernel of the step may be launched while
+// its predecessor drains; it waits here, before touching any memory, until
+// the predecessor has completed and its writes are visible (a no-op for a
+// launch without the attribute).
+__device__ __forceinline__ void wait_for_predecessor() {
+#if GBH_PDL
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
 
 // Order-preserving float <-> uint mapping (for integer atomics on floats).
 __device__ __forceinline__ uint32_t enc_f32(float f) {
@@ -172,6 +204,7 @@ template <int MODE>
 __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ sims,
                                                    const uint32_t* __restrict__ chunk_sim,
                                                    uint32_t nchunks, uint32_t* minmax) {
+    wait_for_predecessor();
     constexpr bool kBounds = MODE != 2;
     __shared__ uint32_t s_sim[8];
     __shared__ float s_val[8][4];
@@ -289,6 +322,7 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
                                                          const uint32_t* __restrict__ minmax,
                                                          uint32_t* __restrict__ keys,
                                                          uint32_t* hist, SimOut* simout) {
+    wait_for_predecessor();
     constexpr int kPasses = 32 / BITS;
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t sh[kPasses * kDig];
@@ -343,6 +377,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     const uint32_t* __restrict__ hist, uint32_t* flags, const uint32_t* __restrict__ keys_in,
     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, float4* __restrict__ sbody, uint32_t* err) {
+    wait_for_predecessor();
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_whist[8][kDig];
@@ -517,6 +552,7 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
     const SimDesc* __restrict__ sims, const uint32_t* __restrict__ chunk_sim, uint32_t npos,
     const uint32_t* __restrict__ codes, uint32_t* __restrict__ base, uint32_t* tile_counter,
     unsigned long long* flags, uint32_t* err) {
+    wait_for_predecessor();
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[8];
     __shared__ unsigned long long s_excl;
@@ -635,6 +671,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
                                                          uint4* cell_child, uint32_t* cell_parent,
                                                          uint32_t* cell_counter, CellRec* groups,
                                                          uint32_t* err) {
+    wait_for_predecessor();
     __shared__ uint32_t s_code[kCellsWin];
     __shared__ uint32_t s_base[kCellsWin + 1];
     __shared__ uint8_t s_owner[kCellsThreads * kMaxChain];  // cell -> position in block
@@ -930,6 +967,7 @@ constexpr uint32_t kAggThreads = 64;
 __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint32_t npos,
                                                            const uint32_t* __restrict__ base,
                                                            uint32_t* err) {
+    wait_for_predecessor();
     // local internal cells by depth (offsets from kb): one cell per position
     // and depth, internal depths 0..15
     __shared__ uint16_t s_level[kMortonDepth][kAggPositions];
@@ -1104,6 +1142,7 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
     const uint32_t* __restrict__ chunk_sim, uint32_t nchunks, const float4* __restrict__ sbody,
     const CellRec* __restrict__ groups, const double4* __restrict__ cell_d, uint32_t capacity,
     unsigned long long* stats, uint32_t* err) {
+    wait_for_predecessor();
     __shared__ uint2 s_stack[WARPS][kTravStack];  // (node group, lane mask)
     __shared__ float4 s_list[WARPS][kTravList];   // (com_x, com_y, G*m, lane mask bits)
     __shared__ uint4 s_mix[WARPS][32];  // mixed slots: (group, slot, lane mask, opened)
@@ -1642,28 +1681,26 @@ static uint32_t integrate_blocks(uint32_t nchunks) {
 cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s) {
     const uint32_t blocks = integrate_blocks(b.nchunks);
     switch (mode) {
-        case 0: k_integrate<0><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
-        case 1: k_integrate<1><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
-        case 2: k_integrate<2><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
-        default: k_integrate<3><<<blocks, 256, 0, s>>>(b.sims, b.chunk_sim, b.nchunks, b.minmax); break;
+        case 0: return launch_step(k_integrate<0>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        case 1: return launch_step(k_integrate<1>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        case 2: return launch_step(k_integrate<2>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        default: return launch_step(k_integrate<3>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
     }
     return cudaGetLastError();
 }
 
 cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s) {
     if (b.radix_bits == 4)
-        k_morton<4><<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a,
-                                                      b.hist, b.simout);
-    else
-        k_morton<8><<<b.ntiles, kSortThreads, 0, s>>>(b.sims, b.tiles, b.minmax, b.keys_a,
-                                                      b.hist, b.simout);
-    return cudaGetLastError();
+        return launch_step(k_morton<4>, b.ntiles, kSortThreads, 0, s, b.sims, b.tiles, b.minmax,
+                           b.keys_a, b.hist, b.simout);
+    return launch_step(k_morton<8>, b.ntiles, kSortThreads, 0, s, b.sims, b.tiles, b.minmax,
+                       b.keys_a, b.hist, b.simout);
 }
 
 // Passes alternate a -> b -> a ...; an even pass count leaves the sorted keys
 // in keys_a / vals_a, and the last pass also gathers the sorted bodies.
 template <int BITS, int PASS>
-static void radix_passes(const BatchBuffers& b, cudaStream_t s) {
+static cudaError_t radix_passes(const BatchBuffers& b, cudaStream_t s) {
     constexpr int kPasses = 32 / BITS;
     const size_t fstride = (size_t)b.ntiles << BITS;
     const bool even = (PASS % 2) == 0;
@@ -1671,42 +1708,36 @@ static void radix_passes(const BatchBuffers& b, cudaStream_t s) {
     const uint32_t* vin = even ? b.vals_a : b.vals_b;
     uint32_t* kout = even ? b.keys_b : b.keys_a;
     uint32_t* vout = even ? b.vals_b : b.vals_a;
-    k_radix_pass<BITS, PASS, PASS == kPasses - 1><<<b.ntiles, kSortThreads, 0, s>>>(
-        b.sims, b.tiles, b.counters + PASS, b.hist, b.sort_flags + PASS * fstride, kin,
-        PASS == 0 ? nullptr : vin, kout, vout, b.sbody, b.err);
-    if constexpr (PASS + 1 < kPasses) radix_passes<BITS, PASS + 1>(b, s);
+    const cudaError_t e = launch_step(k_radix_pass<BITS, PASS, PASS == kPasses - 1>, b.ntiles,
+                                      kSortThreads, 0, s, b.sims, b.tiles, b.counters + PASS,
+                                      b.hist, b.sort_flags + PASS * fstride, kin,
+                                      PASS == 0 ? nullptr : vin, kout, vout, b.sbody, b.err);
+    if (e != cudaSuccess) return e;
+    if constexpr (PASS + 1 < kPasses) return radix_passes<BITS, PASS + 1>(b, s);
+    return cudaSuccess;
 }
 
 cudaError_t launch_radix(const BatchBuffers& b, cudaStream_t s) {
-    if (b.radix_bits == 4)
-        radix_passes<4, 0>(b, s);
-    else
-        radix_passes<8, 0>(b, s);
-    return cudaGetLastError();
+    return b.radix_bits == 4 ? radix_passes<4, 0>(b, s) : radix_passes<8, 0>(b, s);
 }
 
 cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
-    k_count_scan<<<b.nscan_tiles, kScanThreads, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.keys_a,
-                                                        b.base, b.counters + 8, b.scan_flags,
-                                                        b.err);
-    return cudaGetLastError();
+    return launch_step(k_count_scan, b.nscan_tiles, kScanThreads, 0, s, b.sims, b.chunk_sim,
+                       b.npos, b.keys_a, b.base, b.counters + 8, b.scan_flags, b.err);
 }
 
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
-    k_cells<<<(b.npos + kCellsThreads - 1) / kCellsThreads, kCellsThreads, 0, s>>>(b.sims, b.chunk_sim, b.npos, b.cell_capacity,
-                                                 b.keys_a, b.base, b.cell_r, b.cell_end,
-                                                 b.cell_child, b.cell_parent, b.cell_counter,
-                                                 b.groups, b.err);
-    return cudaGetLastError();
+    return launch_step(k_cells, (b.npos + kCellsThreads - 1) / kCellsThreads, kCellsThreads, 0, s,
+                       b.sims, b.chunk_sim, b.npos, b.cell_capacity, b.keys_a, b.base, b.cell_r,
+                       b.cell_end, b.cell_child, b.cell_parent, b.cell_counter, b.groups, b.err);
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
     const AggArgs a{b.sims,          b.simout, b.chunk_sim, b.sbody,      b.keys_a,
                     b.cell_capacity, b.cell_r, b.cell_end,  b.cell_child, b.cell_parent,
                     b.cell_counter,  b.cell_d, b.groups};
-    k_aggregate<<<(b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0, s>>>(
-        a, b.npos, b.base, b.err);
-    return cudaGetLastError();
+    return launch_step(k_aggregate, (b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0,
+                       s, a, b.npos, b.base, b.err);
 }
 
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {
@@ -1717,38 +1748,35 @@ cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t
 }
 
 template <int WARPS>
-static void traverse_launch(const BatchBuffers& b, bool compensated, bool potential, bool stats,
-                            cudaStream_t s) {
+static cudaError_t traverse_launch(const BatchBuffers& b, bool compensated, bool potential,
+                                   bool stats, cudaStream_t s) {
     const uint32_t blocks = (b.nchunks + WARPS - 1) / WARPS;
 #define GBH_TRAVERSE(C, P, S)                                                                   \
-    k_traverse<C, P, S, WARPS><<<blocks, WARPS * 32, 0, s>>>(                                \
-        b.sims, b.simout, b.chunk_sim, b.nchunks, b.sbody, b.groups, b.cell_d, b.cell_capacity, \
-        b.force_stats, b.err)
+    return launch_step(k_traverse<C, P, S, WARPS>, blocks, WARPS * 32, 0, s, b.sims, b.simout,  \
+                       b.chunk_sim, b.nchunks, b.sbody, b.groups, b.cell_d, b.cell_capacity,    \
+                       b.force_stats, b.err)
     if (stats) {
         if (compensated) {
-            if (potential) GBH_TRAVERSE(true, true, true); else GBH_TRAVERSE(true, false, true);
-        } else {
-            if (potential) GBH_TRAVERSE(false, true, true); else GBH_TRAVERSE(false, false, true);
+            if (potential) GBH_TRAVERSE(true, true, true);
+            GBH_TRAVERSE(true, false, true);
         }
-    } else {
-        if (compensated) {
-            if (potential) GBH_TRAVERSE(true, true, false); else GBH_TRAVERSE(true, false, false);
-        } else {
-            if (potential) GBH_TRAVERSE(false, true, false); else GBH_TRAVERSE(false, false, false);
-        }
+        if (potential) GBH_TRAVERSE(false, true, true);
+        GBH_TRAVERSE(false, false, true);
     }
+    if (compensated) {
+        if (potential) GBH_TRAVERSE(true, true, false);
+        GBH_TRAVERSE(true, false, false);
+    }
+    if (potential) GBH_TRAVERSE(false, true, false);
+    GBH_TRAVERSE(false, false, false);
 #undef GBH_TRAVERSE
 }
 
 cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
                             cudaStream_t s) {
-    if (b.trav_warps == 2)
-        traverse_launch<2>(b, compensated, potential, stats, s);
-    else if (b.trav_warps == 4)
-        traverse_launch<4>(b, compensated, potential, stats, s);
-    else
-        traverse_launch<kTravWarps>(b, compensated, potential, stats, s);
-    return cudaGetLastError();
+    if (b.trav_warps == 2) return traverse_launch<2>(b, compensated, potential, stats, s);
+    if (b.trav_warps == 4) return traverse_launch<4>(b, compensated, potential, stats, s);
+    return traverse_launch<kTravWarps>(b, compensated, potential, stats, s);
 }
 
 cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,
