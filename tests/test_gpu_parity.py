@@ -456,3 +456,25 @@ def test_forces_on_small_and_degenerate_systems(gpu, rt, oracle, case):
     assert gs["direct_terms"] == stats["direct_terms"]
     rt.step(gpu, ev, tree, cfg, 1e-3, 3)
     assert np.isfinite(gpu.read_evolving_state(ev)[0]).all()
+
+
+@pytest.mark.slow
+def test_large_n_tree_and_sampled_forces(gpu, rt, oracle):
+    """N = 2^23: the whole tree bit-exact (Morton codes, permutation and the
+    topology checksum over every cell), forces of 1,000 sampled bodies within
+    tolerance of the oracle's traversal of the same tree, and fused steps."""
+    n = 1 << 23
+    bodies = scenarios.cold_disc(n, 19)
+    cfg = Config(theta=0.5, softening_kpc=0.005, g=1.0, bucket=1)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    e = evid.entries["data"]
+    assert np.array_equal(e[:, 0], ot.codes) and np.array_equal(e[:, 1], ot.order)
+    assert evid.active_cell_count == len(ot.cells)
+    assert oracle.topology_checksum_arrays(e, evid.cells.view(np.uint32).reshape(-1, 16)) == \
+        ot.checksum
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    targets = np.random.default_rng(1).choice(n, 1000, replace=False).astype(np.uint32)
+    force_check(oracle, acc, b32, ot, oc, targets=targets)
+    rt.step(gpu, ev, tree, cfg, 5e-4, 2)
+    assert np.isfinite(gpu.read_evolving_state(ev)[0]).all()
