@@ -114,7 +114,9 @@ typedef struct {
     uint64_t approximated_cells;
     uint64_t direct_terms;
     uint64_t exact_mac_fallbacks; /* MAC tests decided in f64 (guard band) */
-    uint64_t warp_iterations;     /* cells walked by warps (union of 32 lanes) */
+    uint64_t warp_iterations;     /* warp steps: walk pops of node groups plus the
+                                     lane-by-lane tests of cells whose opening
+                                     differs within a warp */
 } bh_force_stats;
 
 typedef struct bh_device bh_device;

@@ -112,3 +112,11 @@ def test_host_state_validation():
         bodies_to_state(np.zeros((1, 5)) + 1)
     with pytest.raises(ValueError, match="bucket"):
         Config(bucket=0).validate()
+
+
+def test_integration_rust_block_covers_the_header():
+    """INTEGRATION.md's Rust extern blocks declare every function of the
+    header, so a maintainer wiring the runtime binds the whole surface."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    rust = set(re.findall(r"fn (galaxy_bh_[a-z0-9_]+)\(", text))
+    assert set(declared_symbols()) <= rust, sorted(set(declared_symbols()) - rust)
