@@ -227,6 +227,66 @@ def cpu_baseline_sample() -> dict:
                       f"forces {tf:.2f} s)"}
 
 
+def cpu_config1_sample(steps: int = 10) -> dict:
+    """The reference CPU path on config 1 (exponential disc, N = 16,384, eps
+    0.01, theta 0.5, bucket 1, dt 1e-3, seed 42): `steps` single-threaded KDK
+    steps of its C restatement."""
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import bodies_to_state, state_to_bodies
+    from oracle import oracle
+    b = np.ascontiguousarray(state_to_bodies(bodies_to_state(scenarios.exponential_disc(
+        16384, 42, eps=0.01))))
+    cfg = oracle.Config(theta=0.5, softening=0.01, g=1.0, bucket=1, max_depth=48)
+    tree = oracle.build_flat_tree(b, cfg)
+    acc, _ = oracle.flat_accelerations(b, tree, cfg, nthreads=1)
+    acc = np.ascontiguousarray(acc)
+    t0 = time.perf_counter()
+    oracle.cpu_flat_steps(b, acc, steps, 1e-3, cfg, 1)
+    secs = time.perf_counter() - t0
+    return {"value": 16384 * steps / secs, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{steps} of the config's 100 KDK steps, single thread"}
+
+
+def run_config1_leg(gpu, rt) -> dict:
+    """Config 1: rotating exponential disc, N = 16,384, total mass 1, G 1,
+    eps 0.01, theta 0.5, bucket 1, 100 KDK steps at dt 1e-3 from seed 42;
+    FP64 direct-sum error of the final forces at every body."""
+    import numpy as np
+    import torch
+
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import Config
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1, max_depth=48)
+    bodies = scenarios.exponential_disc(16384, 42, eps=0.01)
+    stream = torch.cuda.ExternalStream(gpu.stream_ptr())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    warm, _ = gpu.create_evolving_state(bodies)  # graphs and arena, untimed
+    tw = rt.create_tree(gpu, warm, cfg)
+    rt.rebuild(gpu, warm, tw, cfg)
+    rt.force(gpu, warm, tw, cfg)
+    rt.step(gpu, warm, tw, cfg, 1e-3, 5)
+    tw.close()
+    warm.close()
+    ev, _ = gpu.create_evolving_state(bodies)
+    tree = rt.create_tree(gpu, ev, cfg)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    rt.rebuild(gpu, ev, tree, cfg)  # the boundary solve is part of the run
+    rt.force(gpu, ev, tree, cfg)
+    rt.step(gpu, ev, tree, cfg, 1e-3, 100)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    err = gpu.probe_error(ev, cfg, np.arange(16384, dtype=np.uint32))
+    tree.close()
+    ev.close()
+    return {"workload": "exponential disc N=16384, eps 0.01, theta 0.5, bucket 1, dt 1e-3, "
+                        "seed 42, 100 KDK steps (boundary solve included)",
+            "value": 16384 * 100 / (ms * 1e-3), "unit": METRIC, "ms_per_step": ms / 100,
+            "force_error_all_bodies": err}
+
+
 def run_engine(args, world, rank, local, pg):
     import torch
 
@@ -354,6 +414,7 @@ def run_engine(args, world, rank, local, pg):
     if not args.no_served:
         served = run_served_leg(gpu, capacity=(batched or {}).get("value", value), pg=pg,
                                 rank=rank, world=world)
+    config1 = run_config1_leg(gpu, rt)
     precision = None
     if not args.no_precision:
         precision = run_precision_leg(gpu, steps=args.precision_steps)
@@ -363,6 +424,8 @@ def run_engine(args, world, rank, local, pg):
             pg.destroy_process_group()
         return
     cpu = None if args.no_cpu_baseline else cpu_baseline_sample()
+    if cpu is not None:
+        config1["cpu_baseline"] = cpu_config1_sample()
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
@@ -403,6 +466,7 @@ def run_engine(args, world, rank, local, pg):
         "at_1e-3_force_error": accurate,
         "batched": batched,
         "served": served,
+        "config1": config1,
         "precision": precision,
         "clocks": clk,
         "gpu_launches": 10 * args.steps + 1,
