@@ -444,7 +444,13 @@ def run_engine(args, world, rank, local, pg):
                                 "passes, count/scan, cells, aggregate)",
                      "peak_source": peaks["source"],
                      "algorithmic_bytes_per_body": {k: round(v, 1) for k, v in ab.items()},
-                     "stage_ms": {k: round(v * 1e3, 4) for k, v in stage.items()}},
+                     "stage_ms": {k: round(v * 1e3, 4) for k, v in stage.items()},
+                     # algorithmic bytes / stage time, per stage ("bounds" is the
+                     # leapfrog + bounds kernel): which stages run at bandwidth
+                     "stage_gbs": {k: round(N_BODIES * ab[m] / stage[k] / 1e9, 1) for k, m in
+                                   (("bounds", "integrate"), ("morton", "morton"),
+                                    ("radix", "radix"), ("topology", "topology"),
+                                    ("aggregate", "aggregate")) if stage[k] > 0}},
         "traversal": {"bound": "fp32", "interactions_per_step": interactions,
                       "interactions_per_s": interactions / stage["traverse"],
                       "achieved_tflops": flops / stage["traverse"] / 1e12,
