@@ -35,7 +35,7 @@ import time
 import numpy as np
 
 from . import _lib, presets
-from .nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime, bodies_to_state
+from .nbody_gpu import Config, NbodyGpu, ParallelTreeRuntime
 
 SCHEMA = "galaxy.barnes-hut-parallel-gpu-tree-receipt.v1"
 BUILDER = "gpu-parallel-sparse-radix-v1"

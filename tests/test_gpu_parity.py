@@ -359,7 +359,6 @@ def test_state_upload_and_readback_checks(gpu, oracle):
     and leaves the resident state as it was; read_state reports the first
     record whose values are no longer finite (nbody_gpu.rs:1043-1053)."""
     from galaxy_b200 import _lib
-    import ctypes as C
     bodies = scenarios.exponential_disc(3000, 5)
     ev, _ = gpu.create_evolving_state(bodies)
     s0, _ = gpu.read_evolving_state_records(ev)
