@@ -126,6 +126,53 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class HostNumaBinding:
+    """Binds this process to the host CPUs that NVML lists as local to the GPU.
+
+    Used around the legs that copy host buffers: pinned pages are first touched
+    and copies issued from the GPU's own NUMA node instead of across the socket
+    link.  A process setting only (sched_setaffinity); the previous CPU set is
+    restored on exit.  Nothing on the GPU changes."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.saved = None
+        self.cpus = None
+
+    def local_cpus(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                p = torch.cuda.get_device_properties(self.device)
+                bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+                words = (os.cpu_count() + 63) // 64
+                mask = pynvml.nvmlDeviceGetCpuAffinity(h, words)
+            finally:
+                pynvml.nvmlShutdown()
+        except Exception:
+            return None
+        cpus = {w * 64 + b for w in range(len(mask)) for b in range(64) if (mask[w] >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+
+    def __enter__(self):
+        self.cpus = self.local_cpus()
+        if self.cpus:
+            self.saved = os.sched_getaffinity(0)
+            os.sched_setaffinity(0, self.cpus)
+        return self
+
+    def __exit__(self, *exc):
+        if self.saved:
+            os.sched_setaffinity(0, self.saved)
+
+    def summary(self) -> dict:
+        return {"bound": bool(self.cpus), "cpus": len(self.cpus) if self.cpus else None}
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -385,22 +432,25 @@ def run_engine(args, world, rank, local, pg):
 
     # --- end to end through the public API with host buffers
     e2e_steps = min(args.steps, 20)
-    pinned = torch.empty(N_BODIES * 32, dtype=torch.uint8, pin_memory=True)
-    host = pinned.numpy().view(_lib.EVOLVE_STATE_DTYPE)
-    gpu_state, _ = gpu.read_evolving_state_records(ev)
-    host[:] = gpu_state
-    L = _lib.load()
-    hp = host.ctypes.data
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        _lib.check(L.galaxy_bh_write_state(gpu.handle, ev.handle, hp, N_BODIES))
-        rt.step(gpu, ev, tree, cfg, DT, 1)
-        _lib.check(L.galaxy_bh_read_state(gpu.handle, ev.handle, hp, N_BODIES, None))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_wall = time.perf_counter() - t0
+    numa = HostNumaBinding(local)
+    with numa:
+        pinned = torch.empty(N_BODIES * 32, dtype=torch.uint8, pin_memory=True)
+        host = pinned.numpy().view(_lib.EVOLVE_STATE_DTYPE)
+        gpu_state, _ = gpu.read_evolving_state_records(ev)
+        host[:] = gpu_state
+        L = _lib.load()
+        hp = host.ctypes.data
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            _lib.check(L.galaxy_bh_write_state(gpu.handle, ev.handle, hp, N_BODIES))
+            rt.step(gpu, ev, tree, cfg, DT, 1)
+            _lib.check(L.galaxy_bh_read_state(gpu.handle, ev.handle, hp, N_BODIES, None))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_wall = time.perf_counter() - t0
+        del host, pinned
     e2e_ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
     e2e_value = world * N_BODIES * e2e_steps / (e2e_ms * 1e-3)
 
@@ -412,8 +462,9 @@ def run_engine(args, world, rank, local, pg):
                                   rank=rank, world=world)
     served = None
     if not args.no_served:
-        served = run_served_leg(gpu, capacity=(batched or {}).get("value", value), pg=pg,
-                                rank=rank, world=world)
+        with HostNumaBinding(local):
+            served = run_served_leg(gpu, capacity=(batched or {}).get("value", value), pg=pg,
+                                    rank=rank, world=world)
     config1 = run_config1_leg(gpu, rt)
     precision = None
     if not args.no_precision:
@@ -466,7 +517,7 @@ def run_engine(args, world, rank, local, pg):
                 "d2h_bytes_per_step": 32 * N_BODIES, "steps": e2e_steps,
                 "how": "per step: galaxy_bh_write_state from pinned host, one fused KDK step, "
                        "galaxy_bh_read_state to pinned host (C ABI)",
-                "wall_s": e2e_wall},
+                "host_numa": numa.summary(), "wall_s": e2e_wall},
         "cpu_baseline": cpu,
         "force_error": force_error,
         "at_1e-3_force_error": accurate,

@@ -365,12 +365,12 @@ constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = (1u << 30) - 1u;
 
 // One stable BITS-wide LSD pass (BITS = 8: 4 passes, 4: 8 passes) over every
-// simulation's keys.  Tiles never cross
-// simulations; within a simulation, tile order is key order and the
-// decoupled look-back adds the digit counts of the preceding tiles.  Items
-// are ranked warp by warp in key order (match_any peers), so equal digits keep
-// their input order: the permutation equals a stable sort by code, as
-// Rust's sort_by_key (nbody/src/flat.rs:233-234).
+// simulation's keys.  Tiles never cross simulations; within a simulation,
+// tile order is key order and the decoupled look-back adds the digit counts
+// of the preceding tiles.  Items are ranked warp by warp in key order (the
+// lanes sharing a digit found with one ballot per digit bit), so equal
+// digits keep their input order: the permutation equals a stable sort by
+// code, as Rust's sort_by_key (nbody/src/flat.rs:233-234).
 template <int BITS, int PASS, bool LAST>
 __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     const SimDesc* __restrict__ sims, const Tile* __restrict__ tiles, uint32_t* tile_counter,
@@ -410,8 +410,14 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = warp * (kSortItems * 32u) + r * 32u + lane;
         const bool valid = idx < tl.count;
-        const uint32_t d = valid ? ((key[r] >> shift) & (kDig - 1u)) : (kDig + lane);
-        const uint32_t peers = __match_any_sync(kFull, d);
+        const uint32_t d = (key[r] >> shift) & (kDig - 1u);
+        // valid lanes holding the same digit: one ballot per digit bit
+        uint32_t peers = __ballot_sync(kFull, valid);
+#pragma unroll
+        for (int bit = 0; bit < BITS; ++bit) {
+            const uint32_t m = __ballot_sync(kFull, (d >> bit) & 1u);
+            peers &= ((d >> bit) & 1u) ? m : ~m;
+        }
         const uint32_t leader = __ffs(peers) - 1u;
         uint32_t b = 0;
         if (valid && lane == leader) {
