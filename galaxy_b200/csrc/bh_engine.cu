@@ -830,10 +830,17 @@ static bool any_flag(Batch* b, uint32_t flag) {
     return false;
 }
 
+static bool any_without_flag(Batch* b, uint32_t flag) {
+    for (auto& c : b->cfgs)
+        if (!(c.flags & flag)) return true;
+    return false;
+}
+
 static int enqueue_force(Batch* b, bool stats) {
     cudaStream_t s = b->dev->stream;
     if (stats) CK(cudaMemsetAsync(b->bb.force_stats, 0, 40, s), "memset");
-    CK(launch_traverse(b->bb, any_flag(b, BH_FLAG_COMPENSATED), any_flag(b, BH_FLAG_POTENTIAL),
+    CK(launch_traverse(b->bb, any_flag(b, BH_FLAG_COMPENSATED),
+                       any_without_flag(b, BH_FLAG_COMPENSATED), any_flag(b, BH_FLAG_POTENTIAL),
                        stats, s),
        "traverse launch");
     return BH_OK;
@@ -861,7 +868,8 @@ static int apply_configs(Batch* b, const bh_config* cfgs, bool for_rebuild) {
 static int run_graphs(Batch* b, uint32_t nsteps) {
     cudaStream_t s = b->dev->stream;
     const uint32_t flags = (any_flag(b, BH_FLAG_COMPENSATED) ? 1u : 0u) |
-                           (any_flag(b, BH_FLAG_POTENTIAL) ? 2u : 0u);
+                           (any_flag(b, BH_FLAG_POTENTIAL) ? 2u : 0u) |
+                           (any_without_flag(b, BH_FLAG_COMPENSATED) ? 4u : 0u);
     if (b->graph_flags != flags) {
         for (auto& g : b->graphs)
             if (g) {

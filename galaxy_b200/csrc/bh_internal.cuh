@@ -124,8 +124,10 @@ cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s);
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s);
 // Recomputes G*m and the MAC bounds of simulation `sim` for new theta / G.
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s);
-cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
-                            cudaStream_t s);
+// One launch per summation form present in the batch (compensated two-sum,
+// plain); each launch computes only the simulations that use its form.
+cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool plain, bool potential,
+                            bool stats, cudaStream_t s);
 cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,
                           GpuCell* cells, cudaStream_t s);
 cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bodies,

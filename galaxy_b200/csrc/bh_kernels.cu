@@ -1159,6 +1159,9 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
     const uint32_t s = chunk_sim[chunk];
     if (s == kNone) return;
     const SimDesc& sd = sims[s];
+    // each instance sums only the simulations that asked for its summation
+    // form, so a simulation's forces do not depend on its batch mates
+    if (((sd.flags & BH_FLAG_COMPENSATED) != 0u) != COMP) return;
     const uint32_t p0 = chunk * kChunk;
     const uint32_t p = p0 + lane;
     const bool valid = p < sd.off + sd.n;
@@ -1778,11 +1781,19 @@ static cudaError_t traverse_launch(const BatchBuffers& b, bool compensated, bool
 #undef GBH_TRAVERSE
 }
 
-cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool potential, bool stats,
-                            cudaStream_t s) {
+static cudaError_t traverse_form(const BatchBuffers& b, bool compensated, bool potential,
+                                 bool stats, cudaStream_t s) {
     if (b.trav_warps == 2) return traverse_launch<2>(b, compensated, potential, stats, s);
     if (b.trav_warps == 4) return traverse_launch<4>(b, compensated, potential, stats, s);
     return traverse_launch<kTravWarps>(b, compensated, potential, stats, s);
+}
+
+cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool plain, bool potential,
+                            bool stats, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    if (compensated) e = traverse_form(b, true, potential, stats, s);
+    if (e == cudaSuccess && plain) e = traverse_form(b, false, potential, stats, s);
+    return e;
 }
 
 cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,

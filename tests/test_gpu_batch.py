@@ -17,7 +17,9 @@ pytestmark = pytest.mark.gpu
 MEMBERS = [
     ("exponential_disc", 1500, 11, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)),
     ("cold_disc", 40000, 12, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=4)),
-    ("binary_encounter", 4097, 13, Config(theta=0.3, softening_kpc=0.005, g=1.0, bucket=1)),
+    # compensated two-sum beside plain members: each keeps its own summation form
+    ("binary_encounter", 4097, 13, Config(theta=0.3, softening_kpc=0.005, g=1.0, bucket=1,
+                                          compensated=True)),
     ("exponential_disc", 70001, 14, Config(theta=0.7, softening_kpc=0.01, g=1.0, bucket=8)),
     ("cold_disc", 33, 15, Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=16)),
 ]
