@@ -260,8 +260,10 @@ int galaxy_bh_conservation_noalloc(const GpuEvolveState* state, const float* pot
 
 /* ---- batched engine --------------------------------------------------------
  * Many independent simulations of uneven n advanced together: one launch per
- * stage covers every simulation.  Each state keeps its own resident buffers;
- * cfgs[i] applies to states[i]. */
+ * stage covers every simulation (the force stage takes one launch per
+ * summation form present, plain and BH_FLAG_COMPENSATED).  Each state keeps
+ * its own resident buffers; cfgs[i] applies to states[i] alone, so a
+ * member's results are bit-identical to the same state advanced by itself. */
 int galaxy_bh_batch_create(bh_device* dev, bh_state* const* states, const bh_config* cfgs,
                            uint32_t count, bh_batch** out);
 int galaxy_bh_batch_destroy(bh_batch* batch);
