@@ -1030,6 +1030,30 @@ extern "C" int galaxy_bh_force_stats(bh_device* dev, bh_tree* tree, bh_force_sta
     return BH_OK;
 }
 
+extern "C" int galaxy_bh_wait_probe(bh_device* dev, uint64_t spin_cycles) {
+    int rc = enter(dev);
+    if (rc) return rc;
+    if (spin_cycles > (uint64_t)4000000000ull)
+        return set_error(BH_INVALID_ARG, "spin_cycles above 4e9 (about two seconds)");
+    // flags of the never-published first tile, the error word, the results
+    constexpr size_t kWords = 2 * kRadixDigits + 1;
+    uint32_t* d = nullptr;
+    CK(cudaMalloc(&d, kWords * 4), "probe allocation");
+    cudaError_t e = cudaMemsetAsync(d, 0, kWords * 4, dev->stream);
+    if (e == cudaSuccess)
+        e = launch_wait_probe(d, d + kRadixDigits, (long long)spin_cycles, d + kRadixDigits + 1,
+                              dev->stream);
+    uint32_t err = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&err, d + kRadixDigits, 4, cudaMemcpyDeviceToHost, dev->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(dev->stream);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "wait probe");
+    if (err & kErrLookbackTimeout)
+        return set_error(BH_TIMEOUT, "device wait (look-back) timed out (error bits 0x%x)", err);
+    return set_error(BH_CUDA_ERROR, "wait probe: the bounded wait did not report its timeout");
+}
+
 extern "C" int galaxy_bh_read_tree_evidence(bh_device* dev, bh_tree* tree, TreeMeta* meta,
                                             GpuEntry* entries, GpuBody* bodies, uint32_t n,
                                             GpuCell* cells, uint32_t cell_capacity,

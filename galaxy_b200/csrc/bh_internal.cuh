@@ -124,6 +124,10 @@ cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s);
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s);
 // Recomputes G*m and the MAC bounds of simulation `sim` for new theta / G.
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s);
+// Bounded-wait probe: the radix look-back against kRadixDigits zeroed flags
+// (a first tile that never publishes); limit in clock cycles, 0 = production.
+cudaError_t launch_wait_probe(const uint32_t* flags, uint32_t* err, long long limit,
+                              uint32_t* out, cudaStream_t s);
 // One launch per summation form present in the batch (compensated two-sum,
 // plain); each launch computes only the simulations that use its form.
 cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool plain, bool potential,

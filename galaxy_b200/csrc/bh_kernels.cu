@@ -364,6 +364,56 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = (1u << 30) - 1u;
 
+// Decoupled look-back of tile t for one digit (flags[tile * stride] holds
+// that tile's state | count): the sum of the predecessors' counts back to the
+// nearest inclusive prefix, reading kLookWindow flags per round trip and
+// re-polling from the first tile that has not published yet.  The
+// simulation's first tile publishes an inclusive prefix at once, so the
+// window never needs tiles before it.  The wait is bounded: past `limit`
+// clock cycles without progress it sets kErrLookbackTimeout and returns the
+// partial sum, which is at most the true prefix (writes stay in range).
+__device__ __forceinline__ uint32_t lookback_digit(const uint32_t* flags, uint32_t stride,
+                                                   uint32_t t, uint32_t first_tile,
+                                                   uint32_t* err, long long limit) {
+    uint32_t excl = 0;
+    uint32_t tp = t - 1;
+    const long long t0 = clock64();
+    while (true) {
+        uint32_t f[kLookWindow];
+#pragma unroll
+        for (int j = 0; j < kLookWindow; ++j)
+            f[j] = tp >= first_tile + j ? ld_volatile(flags + (size_t)(tp - j) * stride) : 0u;
+        bool done = false;
+        int used = 0;
+#pragma unroll
+        for (int j = 0; j < kLookWindow; ++j) {
+            if (done || used < j) continue;
+            const uint32_t st = f[j] & ~kFlagMask;
+            if (st == 0u) continue;
+            excl += f[j] & kFlagMask;
+            used = j + 1;
+            done = st == kFlagInc;
+        }
+        if (done) break;
+        tp -= used;
+        if (used < kLookWindow && clock64() - t0 > limit) {
+            set_err(err, kErrLookbackTimeout);
+            break;
+        }
+    }
+    return excl;
+}
+
+// Failure-detection probe: the sort's look-back wait run as tile 1 of a
+// simulation whose first tile never publishes (flags all zero), one thread
+// per digit, so every thread must give up after `limit` cycles and report
+// the timeout.
+__global__ void k_wait_probe(const uint32_t* flags, uint32_t* err, long long limit,
+                             uint32_t* out) {
+    const uint32_t d = threadIdx.x;
+    out[d] = lookback_digit(flags + d, kRadixDigits, 1u, 0u, err, limit);
+}
+
 // One stable BITS-wide LSD pass (BITS = 8: 4 passes, 4: 8 passes) over every
 // simulation's keys.  Tiles never cross simulations; within a simulation,
 // tile order is key order and the decoupled look-back adds the digit counts
@@ -448,37 +498,7 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_pass(
     if (owner) atomicExch(my_flag, (first ? kFlagInc : kFlagAgg) | run);
     uint32_t excl = 0;
     if (owner && !first) {
-        // look back kLookWindow predecessors per round trip: add aggregates
-        // up to the nearest inclusive prefix; re-poll from the first tile
-        // that has not published yet.  The simulation's first tile is
-        // inclusive, so the window never needs tiles before it.
-        uint32_t tp = t - 1;
-        const long long t0 = clock64();
-        while (true) {
-            uint32_t f[kLookWindow];
-#pragma unroll
-            for (int j = 0; j < kLookWindow; ++j)
-                f[j] = tp >= sd.first_tile + j
-                           ? ld_volatile(flags + (size_t)(tp - j) * kDig + d)
-                           : 0u;
-            bool done = false;
-            int used = 0;
-#pragma unroll
-            for (int j = 0; j < kLookWindow; ++j) {
-                if (done || used < j) continue;
-                const uint32_t st = f[j] & ~kFlagMask;
-                if (st == 0u) continue;
-                excl += f[j] & kFlagMask;
-                used = j + 1;
-                done = st == kFlagInc;
-            }
-            if (done) break;
-            tp -= used;
-            if (used < kLookWindow && clock64() - t0 > kSpinCycles) {
-                set_err(err, kErrLookbackTimeout);
-                break;
-            }
-        }
+        excl = lookback_digit(flags + d, kDig, t, sd.first_tile, err, kSpinCycles);
         atomicExch(my_flag, kFlagInc | (excl + run));
     }
     uint32_t tot;
@@ -1747,6 +1767,12 @@ cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
                     b.cell_counter,  b.cell_d, b.groups};
     return launch_step(k_aggregate, (b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0,
                        s, a, b.npos, b.base, b.err);
+}
+
+cudaError_t launch_wait_probe(const uint32_t* flags, uint32_t* err, long long limit,
+                              uint32_t* out, cudaStream_t s) {
+    k_wait_probe<<<1, kRadixDigits, 0, s>>>(flags, err, limit > 0 ? limit : kSpinCycles, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {

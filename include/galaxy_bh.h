@@ -128,6 +128,13 @@ typedef struct bh_batch bh_batch;
 
 /* Copies the calling thread's last error message; returns its length. */
 size_t galaxy_bh_last_error(char* buf, size_t len);
+/* Failure-detection probe (no reference counterpart): runs the sort's
+ * bounded look-back wait against a predecessor that never publishes, with a
+ * limit of spin_cycles GPU clock cycles (0 = the production limit of 2e9,
+ * about one second; at most 4e9).  Returns BH_TIMEOUT with the same message a
+ * stalled sort reports, and leaves the device handle usable; any other
+ * status means the wait did not give up as designed. */
+int galaxy_bh_wait_probe(bh_device* dev, uint64_t spin_cycles);
 uint32_t galaxy_bh_abi_version(void);
 
 /* ---- device --------------------------------------------------------------
