@@ -1160,6 +1160,7 @@ constexpr uint32_t kTravWarps = GBH_TRAVERSE_WARPS;
 constexpr uint32_t kTravStack = 17u * 32u;
 // Interaction list: flushed once it holds >= 32 entries; a step adds <= 32.
 constexpr uint32_t kTravList = 64u;
+static_assert(kTravList >= 64u, "the mixed cells of a step park in list[32, 64)");
 
 template <bool COMP, bool POT, bool STATS, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWarps / WARPS)
@@ -1171,7 +1172,8 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
     wait_for_predecessor();
     __shared__ uint2 s_stack[WARPS][kTravStack];  // (node group, lane mask)
     __shared__ float4 s_list[WARPS][kTravList];   // (com_x, com_y, G*m, lane mask bits)
-    __shared__ uint4 s_mix[WARPS][32];  // mixed slots: (group, slot, lane mask, opened)
+    __shared__ uint4 s_mix[WARPS][32];  // mixed cells by rank: (lo bits, cell, deciding
+                                        // lanes, opened); their f in list[32 + rank]
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t chunk = blockIdx.x * WARPS + warp;
@@ -1285,28 +1287,31 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
         }
         if (STATS) ++n_iter;
 
-        // mixed cells: every lane of the mask decides for itself, one cell
-        // after the other (records re-read through L1, masks through shared)
+        // mixed cells: every lane of the mask that does not hold the cell
+        // decides for itself, one cell after the other; holding lanes open
+        // it (op).  The record's f waits in the free upper half of the
+        // interaction list (at most 31 entries are pending between steps),
+        // the rest and the masks in s_mix.
         const uint32_t bm = __ballot_sync(kFull, mixed);
         const uint32_t mrank = __popc(bm & lanes_below);
-        if (mixed) s_mix[warp][mrank] = make_uint4(e.x, lane & 3u, A, 0u);
+        if (mixed) {
+            list[32u + mrank] = f;
+            s_mix[warp][mrank] = make_uint4(u.x, u.w, R, 0u);
+        }
         __syncwarp();
         const uint32_t nm = __popc(bm);
         for (uint32_t i = 0; i < nm; ++i) {
-            const uint4 mx = s_mix[warp][i];
-            const CellRec* r = groups + 4ull * mx.x + mx.y;
-            const float4 cf = __ldg(&r->f);
-            const uint4 cu = __ldg(&r->u);
-            const bool active = (mx.z & lane_bit) != 0u;
-            const bool holds = (p - cu.y) < cu.z;
+            const float4 cf = list[32u + i];
+            const uint4 cu = s_mix[warp][i];
+            const bool active = (cu.z & lane_bit) != 0u;
             const float dx = cf.x - tx, dy = cf.y - ty;
             const float d2 = dist2(dx, dy);
-            bool approx = active && !holds && d2 > cf.w;
-            bool open = active && (holds || d2 < __uint_as_float(cu.x));
+            bool approx = active && d2 > cf.w;
+            bool open = active && d2 < __uint_as_float(cu.x);
             const bool undecided = active && !approx && !open;
             if (__any_sync(kFull, undecided)) {
                 if (undecided) {
-                    approx = exact_mac(cell_d, cu.w, tx, ty, simout[s].half,
+                    approx = exact_mac(cell_d, cu.y, tx, ty, simout[s].half,
                                        __float_as_uint(cf.w) & 31u, sd.theta);
                     open = !approx;
                     if (STATS) ++n_exact;
@@ -1321,7 +1326,7 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
             if (STATS) ++n_iter;
         }
         __syncwarp();
-        if (mixed) op = s_mix[warp][mrank].w;
+        if (mixed) op |= s_mix[warp][mrank].w;
 
         // leaves of several bodies: each body summed directly, self excluded
         uint32_t bl = __ballot_sync(kFull, multi);
