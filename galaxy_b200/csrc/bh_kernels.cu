@@ -369,9 +369,10 @@ constexpr uint32_t kFlagMask = (1u << 30) - 1u;
 // nearest inclusive prefix, reading kLookWindow flags per round trip and
 // re-polling from the first tile that has not published yet.  The
 // simulation's first tile publishes an inclusive prefix at once, so the
-// window never needs tiles before it.  The wait is bounded: past `limit`
-// clock cycles without progress it sets kErrLookbackTimeout and returns the
-// partial sum, which is at most the true prefix (writes stay in range).
+// window never needs tiles before it.  The wait is bounded: once `limit`
+// clock cycles have passed since it began and a round finds an unpublished
+// predecessor, it sets kErrLookbackTimeout and returns the partial sum, which
+// is at most the true prefix (the caller's writes stay in range).
 __device__ __forceinline__ uint32_t lookback_digit(const uint32_t* flags, uint32_t stride,
                                                    uint32_t t, uint32_t first_tile,
                                                    uint32_t* err, long long limit) {
