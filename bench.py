@@ -486,6 +486,7 @@ def run_engine(args, world, rank, local, pg):
             served = run_served_leg(gpu, capacity=(batched or {}).get("value", value), pg=pg,
                                     rank=rank, world=world)
     config1 = run_config1_leg(gpu, rt)
+    roofline_large = run_large_roofline(gpu, rt, load_peaks()["hbm_gbs"])
     precision = None
     if not args.no_precision:
         precision = run_precision_leg(gpu, steps=args.precision_steps)
@@ -523,6 +524,8 @@ def run_engine(args, world, rank, local, pg):
                                    (("integrate", "integrate"), ("morton", "morton"),
                                     ("radix", "radix"), ("topology", "topology"),
                                     ("aggregate", "aggregate")) if stage[k] > 0}},
+        # the same stages at 16x the bodies (fewer latency-bound steps)
+        "roofline_n2p24": roofline_large,
         "traversal": {"bound": "fp32", "interactions_per_step": interactions,
                       "interactions_per_s": interactions / stage["traverse"],
                       "achieved_tflops": flops / stage["traverse"] / 1e12,
@@ -855,6 +858,37 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
         "plain_serial": {"particle_steps_per_s": plain, "requests": sat["requests"],
                          "includes": "state upload, tree allocation, boundary solve, steps"},
         "speedup_vs_plain": sat["particle_steps_per_s"] / plain if plain else None}
+
+
+def run_large_roofline(gpu, rt, peak_gbs: float, n: int = 1 << 24, reps: int = 3) -> dict:
+    """The sort/build/leapfrog stages of the same workload at N = 2^24 (cold
+    uniform disc, seed 7): the kernels of the 2^20 headline with 16x the
+    bodies, where fewer of their steps are latency-bound.  Device stage times
+    from instrumented rebuilds (mean of `reps`) and the step's kick/drift +
+    bounds kernel on the same state; algorithmic bytes as at 2^20."""
+    from galaxy_b200 import scenarios
+    from galaxy_b200.nbody_gpu import Config, bodies_to_state
+    cfg = Config(theta=THETA, softening_kpc=EPS, g=G, bucket=BUCKET, max_depth=48)
+    s0 = bodies_to_state(scenarios.cold_disc(n, SEED))
+    ev, _ = gpu.create_evolving_state_records(s0)
+    tree = rt.create_tree(gpu, ev, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    stage = {"integrate": 0.0, "morton": 0.0, "radix": 0.0, "topology": 0.0, "aggregate": 0.0}
+    for _ in range(reps):
+        stage["integrate"] += gpu.kick_drift(ev, DT).dispatch_seconds / reps
+        bt = rt.rebuild(gpu, ev, tree, cfg)
+        for k in ("morton", "radix", "topology", "aggregate"):
+            stage[k] += getattr(bt, k + "_seconds") / reps
+    c = tree_cells(gpu, rt, tree) / n
+    tree.close()
+    ev.close()
+    ab = algorithmic_bytes(c)
+    secs = sum(stage.values())
+    achieved = n * sum(ab.values()) / secs / 1e9
+    return {"n_bodies": n, "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+            "frac": achieved / peak_gbs, "cells_per_body": c,
+            "stage_ms": {k: round(v * 1e3, 4) for k, v in stage.items()},
+            "stage_gbs": {k: round(n * ab[k] / v / 1e9, 1) for k, v in stage.items() if v > 0}}
 
 
 def tree_cells(gpu, rt, tree) -> int:
