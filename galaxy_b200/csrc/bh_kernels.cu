@@ -702,6 +702,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
     __shared__ uint32_t s_code[kCellsWin];
     __shared__ uint32_t s_base[kCellsWin + 1];
     __shared__ uint8_t s_owner[kCellsThreads * kMaxChain];  // cell -> position in block
+    __shared__ uint16_t s_end[kCellsThreads * kMaxChain];   // cell -> min(end - P0, 0xffff)
     const uint32_t t = threadIdx.x;
     const uint32_t P0 = blockIdx.x * kCellsThreads;
     for (uint32_t j = t; j <= kCellsWin; j += kCellsThreads) {
@@ -723,19 +724,27 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
     __syncthreads();
     const CellsWindow w{s_code, s_base, codes, base, P0};
     const uint4 absent = make_uint4(0u, 0u, 0u, kNone);  // u.z == 0: no child in this slot
-    for (uint32_t k = kb + t; k < ke; k += kCellsThreads) {
+    // Position, depth and deepest chain depth of cell k of this block.
+    auto locate = [&](uint32_t k, uint32_t* p, uint32_t* d, uint32_t* deepest) {
         const uint32_t tl = s_owner[k - kb];
-        const uint32_t p = P0 + tl;
+        *p = P0 + tl;
+        const SimDesc& sd = sims[chunk_sim[*p >> 5]];
+        const uint32_t ci = s_code[tl];
+        const uint32_t dmin = *p == sd.off
+                                  ? 0u
+                                  : shared_levels(tl ? s_code[tl - 1u] : codes[*p - 1u], ci) + 1u;
+        const uint32_t k0 = s_base[tl];
+        *deepest = dmin + (s_base[tl + 1] - k0) - 1u;
+        *d = dmin + (k - k0);
+    };
+    // Pass 1: every cell's range end (one search each).
+    for (uint32_t k = kb + t; k < ke; k += kCellsThreads) {
+        uint32_t p, d, deepest;
+        locate(k, &p, &d, &deepest);
         const uint32_t s = chunk_sim[p >> 5];
         const SimDesc& sd = sims[s];
-        const uint32_t i = p - sd.off;
         const uint32_t hi = sd.off + sd.n;
-        const uint32_t ci = s_code[tl];
-        const uint32_t dmin =
-            i == 0 ? 0u : shared_levels(tl ? s_code[tl - 1u] : codes[p - 1u], ci) + 1u;
-        const uint32_t k0 = s_base[tl];
-        const uint32_t deepest = dmin + (s_base[tl + 1] - k0) - 1u;
-        const uint32_t d = dmin + (k - k0);
+        const uint32_t ci = s_code[p - P0];
         // end of the depth-d group holding p
         uint32_t end = hi;
         if (d > 0) {
@@ -754,31 +763,60 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
         cell_r[k].u = make_uint4(0u, w.base_at(end), p, d);
         cell_end[k] = end;
         cell_counter[k] = 0;
+        s_end[k - kb] = (uint16_t)min(end - P0, 0xffffu);
+    }
+    __syncthreads();
+    // Pass 2: children.  Children of (p, d) are the depth-(d+1) groups of its
+    // range in position order (= quadrant order): (p, d+1) first, then the
+    // chain head at each child's end.  While those ends lie in this block
+    // they come from pass 1; otherwise the quadrant bounds are searched.
+    for (uint32_t k = kb + t; k < ke; k += kCellsThreads) {
+        uint32_t p, d, deepest;
+        locate(k, &p, &d, &deepest);
         uint4 ch = make_uint4(kNone, kNone, kNone, kNone);
+        uint32_t* chp = &ch.x;
         if (d < deepest) {
+            const uint32_t end = cell_end[k];
             const uint32_t sh = 30u - 2u * d;
-            const uint32_t pre = d == 0 ? 0u : (ci >> (32u - 2u * d));
-            uint32_t bounds[5];
-            bounds[0] = p;
-            uint32_t lo = p;
-#pragma unroll
-            for (uint32_t q = 1; q < 4; ++q) {
-                lo = w.lower_bound(lo, end, ((pre << 2) | q) << sh);
-                bounds[q] = lo;
+            uint32_t q = p, child = k + 1u;
+            bool searched = false;
+            while (true) {
+                chp[(s_code[q - P0] >> sh) & 3u] = child;
+                const uint32_t e = s_end[child - kb];
+                if (P0 + e >= end) break;        // the last child
+                if (e >= P1 - P0) {              // next child starts past this block
+                    searched = true;
+                    break;
+                }
+                q = P0 + e;
+                child = s_base[e];               // chain head of position q
             }
-            bounds[4] = end;
-            uint32_t* chp = &ch.x;
+            if (searched) {
+                const uint32_t pre = d == 0 ? 0u : (s_code[p - P0] >> (32u - 2u * d));
+                uint32_t bounds[5];
+                bounds[0] = p;
+                uint32_t lo = p;
 #pragma unroll
-            for (uint32_t q = 0; q < 4; ++q) {
-                if (bounds[q] < bounds[q + 1]) {
-                    const uint32_t child = bounds[q] == p ? k + 1u : w.base_at(bounds[q]);
-                    chp[q] = child;
-                    if (child < capacity)
-                        cell_parent[child] = k;
-                    else
-                        set_err(err, kErrCapacity);
+                for (uint32_t qd = 1; qd < 4; ++qd) {
+                    lo = w.lower_bound(lo, end, ((pre << 2) | qd) << sh);
+                    bounds[qd] = lo;
+                }
+                bounds[4] = end;
+#pragma unroll
+                for (uint32_t qd = 0; qd < 4; ++qd)
+                    chp[qd] = bounds[qd] < bounds[qd + 1]
+                                  ? (bounds[qd] == p ? k + 1u : w.base_at(bounds[qd]))
+                                  : kNone;
+            }
+#pragma unroll
+            for (uint32_t qd = 0; qd < 4; ++qd) {
+                const uint32_t child = chp[qd];
+                if (child == kNone) {
+                    groups[4ull * k + qd].u = absent;
+                } else if (child < capacity) {
+                    cell_parent[child] = k;
                 } else {
-                    groups[4ull * k + q].u = absent;
+                    set_err(err, kErrCapacity);
                 }
             }
         }
