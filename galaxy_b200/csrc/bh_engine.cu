@@ -597,11 +597,11 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Byte sizes of the arena regions, in carve order.
 struct ArenaPlan {
-    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_r, groups,
+    size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_u, groups,
         cell_end, cell_d, cell_child, cell_parent, cell_counter, err, stats;
     size_t total() const {
         return control + sims + simout + chunk + tiles + 2 * keys + 2 * vals + sbody + base +
-               cell_r + groups + cell_end + cell_d + cell_child + cell_parent + cell_counter +
+               cell_u + groups + cell_end + cell_d + cell_child + cell_parent + cell_counter +
                err + stats;
     }
 };
@@ -619,7 +619,7 @@ static ArenaPlan plan_arena(const Layout& L, uint32_t nsims) {
     a.vals = align256(4ull * L.npos);
     a.sbody = align256(16ull * L.npos);
     a.base = align256(4ull * (L.npos + 1));
-    a.cell_r = align256(sizeof(CellRec) * L.cells);
+    a.cell_u = align256(sizeof(uint4) * L.cells);
     a.groups = align256(4ull * sizeof(CellRec) * (L.cells + nsims));
     a.cell_end = align256(4ull * L.cells);
     a.cell_d = align256(32ull * L.cells);
@@ -719,7 +719,7 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.vals_b = (uint32_t*)take(A.vals);
     bb.sbody = (float4*)take(A.sbody);
     bb.base = (uint32_t*)take(A.base);
-    bb.cell_r = (CellRec*)take(A.cell_r);
+    bb.cell_u = (uint4*)take(A.cell_u);
     bb.groups = (CellRec*)take(A.groups);
     bb.cell_end = (uint32_t*)take(A.cell_end);
     bb.cell_d = (double4*)take(A.cell_d);

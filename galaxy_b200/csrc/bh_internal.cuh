@@ -56,12 +56,14 @@ struct SimOut {
     double reserved;
 };
 
-// Traversal record of one cell (32 bytes, one sector):
+// Traversal record of one cell, its slot in the parent's node group
+// (32 bytes, one sector):
 //   f = (com_x, com_y, G*mass, hi) in f32, with the cell depth in the low 5
 //       bits of hi (hi rounded up to make room, so the MAC band only widens)
-//   u = (lo as f32 bits | leaf body count, skip, start, depth)
+//   u = (lo as f32 bits | leaf body count, start, body count, cell index or
+//       kNone for a leaf)
 // hi is -1 for a one-body leaf and +inf (a NaN once depth is packed) for a
-// leaf of several bodies; skip = index of the next cell after the subtree.
+// leaf of several bodies.  An empty slot has u.z == 0.
 struct CellRec {
     float4 f;
     uint4 u;
@@ -101,7 +103,8 @@ struct BatchBuffers {
     uint32_t* vals_b;
     float4* sbody;      // sorted (x, y, m, body index bits)
     uint32_t* base;     // npos + 1: first cell index of each position's chain
-    CellRec* cell_r;    // per-cell records in preorder (build, export, refresh)
+    uint4* cell_u;      // per cell in preorder: (0, skip, start, depth) (build, export,
+                        // refresh); the MAC fields live in the node-group slots
     CellRec* groups;    // node groups: children of cell k at [4k, 4k+4); simulation s's
                         // root at slot 0 of group cell_capacity + s (traversal)
     uint32_t* cell_end; // end position (build and export only)

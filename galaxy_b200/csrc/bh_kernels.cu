@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
                                                          uint32_t npos, uint32_t capacity,
                                                          const uint32_t* __restrict__ codes,
                                                          const uint32_t* __restrict__ base,
-                                                         CellRec* cell_r, uint32_t* cell_end,
+                                                         uint4* cell_u, uint32_t* cell_end,
                                                          uint4* cell_child, uint32_t* cell_parent,
                                                          uint32_t* cell_counter, CellRec* groups,
                                                          uint32_t* err) {
@@ -759,8 +759,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
             rg[2].u = absent;
             rg[3].u = absent;
         }
-        // u.x (MAC lower bound or leaf body count) and f are filled by k_aggregate
-        cell_r[k].u = make_uint4(0u, w.base_at(end), p, d);
+        cell_u[k] = make_uint4(0u, w.base_at(end), p, d);
         cell_end[k] = end;
         cell_counter[k] = 0;
         s_end[k - kb] = (uint16_t)min(end - P0, 0xffffu);
@@ -880,14 +879,14 @@ __device__ __forceinline__ CellRec* slot_of(CellRec* groups, const SlotRef& r) {
     return groups + (r.parent == kNone ? 4ull * r.root_group : 4ull * r.parent + r.quadrant);
 }
 
-// Writes the MAC fields of cell k into its preorder record and into its slot
-// of the parent's node group: internal cells get (hi|depth, lo); a leaf
+// Writes the MAC fields of cell k into its slot of the parent's node group
+// (the traversal's record of the cell): internal cells get (hi|depth, lo); a leaf
 // (count >= 1 bodies) is always summed directly: one body -> hi = -1 (it
 // passes as a point mass at its own position, which is its f32 centre of
 // mass exactly); several bodies -> hi = +inf (no point-mass term), summed
 // body by body.  The slot's u = (lo | body count, start, body count, k or
 // kNone for a leaf).
-__device__ __forceinline__ void store_mac_fields(CellRec* cell_r, CellRec* groups, uint32_t k,
+__device__ __forceinline__ void store_mac_fields(CellRec* groups, uint32_t k,
                                                  float fx, float fy, float gm, uint32_t depth,
                                                  uint32_t start, uint32_t count, bool leaf,
                                                  const SlotRef& slot, double root_half,
@@ -903,8 +902,6 @@ __device__ __forceinline__ void store_mac_fields(CellRec* cell_r, CellRec* group
         ux = __float_as_uint(lo);
     }
     const float4 f = make_float4(fx, fy, gm, pack_depth(hi, depth));
-    cell_r[k].f = f;
-    reinterpret_cast<uint32_t*>(&cell_r[k].u)[0] = ux;
     CellRec* sl = slot_of(groups, slot);
     sl->f = f;
     sl->u = make_uint4(ux, start, count, leaf ? kNone : k);
@@ -916,12 +913,11 @@ __device__ __forceinline__ void store_cell_values(uint32_t k, double mass, doubl
                                                   uint32_t depth, uint32_t start, uint32_t count,
                                                   bool leaf, const SlotRef& slot,
                                                   double root_half, double theta, float g,
-                                                  double4* cell_d, CellRec* cell_r,
-                                                  CellRec* groups) {
+                                                  double4* cell_d, CellRec* groups) {
     const double com_x = __ddiv_rn(wx, mass);
     const double com_y = __ddiv_rn(wy, mass);
     cell_d[k] = make_double4(com_x, com_y, mass, 0.0);
-    store_mac_fields(cell_r, groups, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass),
+    store_mac_fields(groups, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass),
                      depth, start, count, leaf, slot, root_half, theta);
 }
 
@@ -956,7 +952,7 @@ struct AggArgs {
     const float4* sbody;
     const uint32_t* codes;
     uint32_t capacity;
-    CellRec* cell_r;
+    const uint4* cell_u;
     const uint32_t* cell_end;
     const uint4* cell_child;
     const uint32_t* cell_parent;
@@ -996,7 +992,7 @@ __device__ __forceinline__ void aggregate_cell(const AggArgs& a, uint32_t k, uin
     }
     store_cell_values(k, mass, wx, wy, depth, start, end - start, leaf,
                       slot_ref(a.cell_parent[k], depth, a.codes[start], a.capacity + s),
-                      a.simout[s].half, sd.theta, sd.g_f, a.cell_d, a.cell_r, a.groups);
+                      a.simout[s].half, sd.theta, sd.g_f, a.cell_d, a.groups);
 }
 
 // Cell k is done and its parent spans several blocks: count k in at the
@@ -1010,7 +1006,7 @@ __device__ void climb(const AggArgs& a, uint32_t k) {
         const uint32_t nchild =
             (ch.x != kNone) + (ch.y != kNone) + (ch.z != kNone) + (ch.w != kNone);
         if (atomic_add_acq_rel(a.cell_counter + par, 1u) + 1u != nchild) return;
-        aggregate_cell(a, par, a.cell_r[par].u, false);
+        aggregate_cell(a, par, a.cell_u[par], false);
         k = par;
     }
 }
@@ -1058,7 +1054,7 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
         return left && right;
     };
     for (uint32_t k = kb + t; k < ke; k += kAggThreads) {
-        const uint4 u = a.cell_r[k].u;  // (0, skip, start, depth)
+        const uint4 u = a.cell_u[k];  // (0, skip, start, depth)
         const SimDesc& sd = a.sims[a.chunk_sim[u.z >> 5]];
         if (u.y == k + 1u) {
             aggregate_cell(a, k, u, true);
@@ -1078,7 +1074,7 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
         if (cnt == 0) continue;
         for (uint32_t j = t; j < cnt; j += kAggThreads) {
             const uint32_t k = kb + s_level[d][j];
-            const uint4 u = a.cell_r[k].u;
+            const uint4 u = a.cell_u[k];
             aggregate_cell(a, k, u, false);
             if (d > 0 && !inside(u.z, (uint32_t)d - 1u, a.sims[a.chunk_sim[u.z >> 5]])) climb(a, k);
         }
@@ -1093,18 +1089,17 @@ __global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __
                               const uint32_t* __restrict__ codes, uint32_t capacity,
                               const uint32_t* __restrict__ cell_end,
                               const uint32_t* __restrict__ cell_parent,
-                              const double4* __restrict__ cell_d, CellRec* cell_r,
-                              CellRec* groups) {
+                              const double4* __restrict__ cell_d,
+                              const uint4* __restrict__ cell_u, CellRec* groups) {
     const SimDesc& sd = sims[sim];
     const uint32_t cb = base[sd.off], ce = base[sd.off + sd.n];
     const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ce) return;
-    const uint4 u = cell_r[k].u;
-    const float4 f = cell_r[k].f;
+    const uint4 u = cell_u[k];
     const double4 v = cell_d[k];
     const bool leaf = u.y == k + 1u;
     const uint32_t start = u.z;
-    store_mac_fields(cell_r, groups, k, f.x, f.y, __fmul_rn(sd.g_f, (float)v.z), u.w, start,
+    store_mac_fields(groups, k, (float)v.x, (float)v.y, __fmul_rn(sd.g_f, (float)v.z), u.w, start,
                      cell_end[k] - start, leaf,
                      slot_ref(cell_parent[k], u.w, codes[start], capacity + sim),
                      simout[sim].half, sd.theta);
@@ -1552,7 +1547,7 @@ __global__ void __launch_bounds__(256) k_traverse_packed(
 __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
                                uint32_t sim, const uint32_t* __restrict__ codes,
                                const uint32_t* __restrict__ base,
-                               const CellRec* __restrict__ cell_r,
+                               const uint4* __restrict__ cell_u,
                                const uint32_t* __restrict__ cell_end,
                                const uint4* __restrict__ cell_child,
                                const double4* __restrict__ cell_d, GpuCell* out) {
@@ -1561,7 +1556,7 @@ __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* _
     const uint32_t k = cb + blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= ce) return;
     const SimOut so = simout[sim];
-    const uint4 u = cell_r[k].u;
+    const uint4 u = cell_u[k];
     const uint32_t start = u.z - sd.off;
     const uint32_t code = codes[u.z];
     double cx = so.cx, cy = so.cy, half = so.half;
@@ -1801,13 +1796,13 @@ cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
 
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
     return launch_step(k_cells, (b.npos + kCellsThreads - 1) / kCellsThreads, kCellsThreads, 0, s,
-                       b.sims, b.chunk_sim, b.npos, b.cell_capacity, b.keys_a, b.base, b.cell_r,
+                       b.sims, b.chunk_sim, b.npos, b.cell_capacity, b.keys_a, b.base, b.cell_u,
                        b.cell_end, b.cell_child, b.cell_parent, b.cell_counter, b.groups, b.err);
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
     const AggArgs a{b.sims,          b.simout, b.chunk_sim, b.sbody,      b.keys_a,
-                    b.cell_capacity, b.cell_r, b.cell_end,  b.cell_child, b.cell_parent,
+                    b.cell_capacity, b.cell_u, b.cell_end,  b.cell_child, b.cell_parent,
                     b.cell_counter,  b.cell_d, b.groups};
     return launch_step(k_aggregate, (b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0,
                        s, a, b.npos, b.base, b.err);
@@ -1822,7 +1817,7 @@ cudaError_t launch_wait_probe(const uint32_t* flags, uint32_t* err, long long li
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {
     k_refresh_mac<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
         b.sims, b.simout, sim, b.base, b.keys_a, b.cell_capacity, b.cell_end, b.cell_parent,
-        b.cell_d, b.cell_r, b.groups);
+        b.cell_d, b.cell_u, b.groups);
     return cudaGetLastError();
 }
 
@@ -1870,7 +1865,7 @@ cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries
                           GpuCell* cells, cudaStream_t s) {
     if (cells)
         k_export_cells<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
-            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_r, b.cell_end, b.cell_child, b.cell_d,
+            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_u, b.cell_end, b.cell_child, b.cell_d,
             cells);
     if (entries || bodies)
         k_export_entries<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, sim, b.keys_a, b.sbody,
