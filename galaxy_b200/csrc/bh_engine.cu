@@ -598,10 +598,10 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // Byte sizes of the arena regions, in carve order.
 struct ArenaPlan {
     size_t control, sims, simout, chunk, tiles, keys, vals, sbody, base, cell_u, groups,
-        cell_end, cell_d, cell_child, cell_parent, cell_counter, err, stats;
+        cell_d, cell_child, cell_parent, cell_counter, err, stats;
     size_t total() const {
         return control + sims + simout + chunk + tiles + 2 * keys + 2 * vals + sbody + base +
-               cell_u + groups + cell_end + cell_d + cell_child + cell_parent + cell_counter +
+               cell_u + groups + cell_d + cell_child + cell_parent + cell_counter +
                err + stats;
     }
 };
@@ -621,7 +621,6 @@ static ArenaPlan plan_arena(const Layout& L, uint32_t nsims) {
     a.base = align256(4ull * (L.npos + 1));
     a.cell_u = align256(sizeof(uint4) * L.cells);
     a.groups = align256(4ull * sizeof(CellRec) * (L.cells + nsims));
-    a.cell_end = align256(4ull * L.cells);
     a.cell_d = align256(32ull * L.cells);
     a.cell_child = align256(16ull * L.cells);
     a.cell_parent = align256(4ull * L.cells);
@@ -721,7 +720,6 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     bb.base = (uint32_t*)take(A.base);
     bb.cell_u = (uint4*)take(A.cell_u);
     bb.groups = (CellRec*)take(A.groups);
-    bb.cell_end = (uint32_t*)take(A.cell_end);
     bb.cell_d = (double4*)take(A.cell_d);
     bb.cell_child = (uint4*)take(A.cell_child);
     bb.cell_parent = (uint32_t*)take(A.cell_parent);

@@ -103,11 +103,10 @@ struct BatchBuffers {
     uint32_t* vals_b;
     float4* sbody;      // sorted (x, y, m, body index bits)
     uint32_t* base;     // npos + 1: first cell index of each position's chain
-    uint4* cell_u;      // per cell in preorder: (0, skip, start, depth) (build, export,
+    uint4* cell_u;      // per cell in preorder: (end, skip, start, depth) (build, export,
                         // refresh); the MAC fields live in the node-group slots
     CellRec* groups;    // node groups: children of cell k at [4k, 4k+4); simulation s's
                         // root at slot 0 of group cell_capacity + s (traversal)
-    uint32_t* cell_end; // end position (build and export only)
     double4* cell_d;    // com_x, com_y, mass, 0 (f64)
     uint4* cell_child;  // children (global cell indices)
     uint32_t* cell_parent;

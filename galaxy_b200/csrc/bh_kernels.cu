@@ -661,6 +661,9 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
 // bases of the next kCellsWin positions sit in shared memory, so the range
 // searches of almost every cell (all but the few that span more than the
 // window) never touch global memory.
+// Positions per k_aggregate block: cells whose range crosses a multiple of it
+// are finished by cross-block climbs (the only users of the cell counters).
+constexpr uint32_t kAggBlockPositions = 256;
 constexpr uint32_t kCellsThreads = 256;
 constexpr uint32_t kCellsWin = 1024;
 constexpr uint32_t kMaxChain = kMortonDepth + 1;  // cells per position: depths 0..16
@@ -694,7 +697,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
                                                          uint32_t npos, uint32_t capacity,
                                                          const uint32_t* __restrict__ codes,
                                                          const uint32_t* __restrict__ base,
-                                                         uint4* cell_u, uint32_t* cell_end,
+                                                         uint4* cell_u,
                                                          uint4* cell_child, uint32_t* cell_parent,
                                                          uint32_t* cell_counter, CellRec* groups,
                                                          uint32_t* err) {
@@ -759,9 +762,9 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
             rg[2].u = absent;
             rg[3].u = absent;
         }
-        cell_u[k] = make_uint4(0u, w.base_at(end), p, d);
-        cell_end[k] = end;
-        cell_counter[k] = 0;
+        cell_u[k] = make_uint4(end, w.base_at(end), p, d);
+        // counters serve only cells that span aggregate blocks (cross-block climbs)
+        if ((p / kAggBlockPositions) != ((end - 1u) / kAggBlockPositions)) cell_counter[k] = 0;
         s_end[k - kb] = (uint16_t)min(end - P0, 0xffffu);
     }
     __syncthreads();
@@ -775,7 +778,7 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
         uint4 ch = make_uint4(kNone, kNone, kNone, kNone);
         uint32_t* chp = &ch.x;
         if (d < deepest) {
-            const uint32_t end = cell_end[k];
+            const uint32_t end = cell_u[k].x;
             const uint32_t sh = 30u - 2u * d;
             uint32_t q = p, child = k + 1u;
             bool searched = false;
@@ -953,7 +956,6 @@ struct AggArgs {
     const uint32_t* codes;
     uint32_t capacity;
     const uint4* cell_u;
-    const uint32_t* cell_end;
     const uint4* cell_child;
     const uint32_t* cell_parent;
     uint32_t* cell_counter;
@@ -965,7 +967,7 @@ struct AggArgs {
 // sums its bodies in Morton order, an internal cell its children in quadrant
 // order 0..3 (nbody/src/flat.rs:179-215).
 __device__ __forceinline__ void aggregate_cell(const AggArgs& a, uint32_t k, uint4 u, bool leaf) {
-    const uint32_t start = u.z, depth = u.w, end = a.cell_end[k];
+    const uint32_t start = u.z, depth = u.w, end = u.x;
     const uint32_t s = a.chunk_sim[start >> 5];
     const SimDesc& sd = a.sims[s];
     double mass = 0.0, wx = 0.0, wy = 0.0;
@@ -1022,7 +1024,7 @@ __device__ void climb(const AggArgs& a, uint32_t k) {
 // reference, so the f64 mass and centre of mass equal its values bit for bit.
 // 64 threads per 256 positions: a depth holds few cells, and small blocks
 // let many blocks hide each other's per-depth latency.
-constexpr uint32_t kAggPositions = 256;
+constexpr uint32_t kAggPositions = kAggBlockPositions;
 constexpr uint32_t kAggThreads = 64;
 
 __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint32_t npos,
@@ -1087,7 +1089,6 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
 __global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout,
                               uint32_t sim, const uint32_t* __restrict__ base,
                               const uint32_t* __restrict__ codes, uint32_t capacity,
-                              const uint32_t* __restrict__ cell_end,
                               const uint32_t* __restrict__ cell_parent,
                               const double4* __restrict__ cell_d,
                               const uint4* __restrict__ cell_u, CellRec* groups) {
@@ -1100,7 +1101,7 @@ __global__ void k_refresh_mac(const SimDesc* __restrict__ sims, const SimOut* __
     const bool leaf = u.y == k + 1u;
     const uint32_t start = u.z;
     store_mac_fields(groups, k, (float)v.x, (float)v.y, __fmul_rn(sd.g_f, (float)v.z), u.w, start,
-                     cell_end[k] - start, leaf,
+                     u.x - start, leaf,
                      slot_ref(cell_parent[k], u.w, codes[start], capacity + sim),
                      simout[sim].half, sd.theta);
 }
@@ -1548,7 +1549,6 @@ __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* _
                                uint32_t sim, const uint32_t* __restrict__ codes,
                                const uint32_t* __restrict__ base,
                                const uint4* __restrict__ cell_u,
-                               const uint32_t* __restrict__ cell_end,
                                const uint4* __restrict__ cell_child,
                                const double4* __restrict__ cell_d, GpuCell* out) {
     const SimDesc& sd = sims[sim];
@@ -1579,7 +1579,7 @@ __global__ void k_export_cells(const SimDesc* __restrict__ sims, const SimOut* _
     c.com[2] = 0.f;
     c.com[3] = 0.f;
     c.range_depth[0] = start;
-    c.range_depth[1] = cell_end[k] - sd.off;
+    c.range_depth[1] = u.x - sd.off;
     c.range_depth[2] = u.w;
     c.range_depth[3] = 0u;
     c.children[0] = ch.x == kNone ? kNone : ch.x - cb;
@@ -1797,12 +1797,12 @@ cudaError_t launch_count_scan(const BatchBuffers& b, cudaStream_t s) {
 cudaError_t launch_cells(const BatchBuffers& b, cudaStream_t s) {
     return launch_step(k_cells, (b.npos + kCellsThreads - 1) / kCellsThreads, kCellsThreads, 0, s,
                        b.sims, b.chunk_sim, b.npos, b.cell_capacity, b.keys_a, b.base, b.cell_u,
-                       b.cell_end, b.cell_child, b.cell_parent, b.cell_counter, b.groups, b.err);
+                       b.cell_child, b.cell_parent, b.cell_counter, b.groups, b.err);
 }
 
 cudaError_t launch_aggregate(const BatchBuffers& b, cudaStream_t s) {
     const AggArgs a{b.sims,          b.simout, b.chunk_sim, b.sbody,      b.keys_a,
-                    b.cell_capacity, b.cell_u, b.cell_end,  b.cell_child, b.cell_parent,
+                    b.cell_capacity, b.cell_u, b.cell_child, b.cell_parent,
                     b.cell_counter,  b.cell_d, b.groups};
     return launch_step(k_aggregate, (b.npos + kAggPositions - 1) / kAggPositions, kAggThreads, 0,
                        s, a, b.npos, b.base, b.err);
@@ -1816,7 +1816,7 @@ cudaError_t launch_wait_probe(const uint32_t* flags, uint32_t* err, long long li
 
 cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t s) {
     k_refresh_mac<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
-        b.sims, b.simout, sim, b.base, b.keys_a, b.cell_capacity, b.cell_end, b.cell_parent,
+        b.sims, b.simout, sim, b.base, b.keys_a, b.cell_capacity, b.cell_parent,
         b.cell_d, b.cell_u, b.groups);
     return cudaGetLastError();
 }
@@ -1865,7 +1865,7 @@ cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries
                           GpuCell* cells, cudaStream_t s) {
     if (cells)
         k_export_cells<<<(b.cell_capacity + 255) / 256, 256, 0, s>>>(
-            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_u, b.cell_end, b.cell_child, b.cell_d,
+            b.sims, b.simout, sim, b.keys_a, b.base, b.cell_u, b.cell_child, b.cell_d,
             cells);
     if (entries || bodies)
         k_export_entries<<<(b.npos + 255) / 256, 256, 0, s>>>(b.sims, sim, b.keys_a, b.sbody,
