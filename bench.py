@@ -37,7 +37,7 @@ THETA, EPS, G, BUCKET, DT, SEED = 0.5, 0.005, 1.0, 1, 5e-4, 7
 METRIC = "particle-steps/s"
 # ncu DRAM bytes (read + write) of integrate, Morton, 4 radix passes, count/scan,
 # cells and aggregate for one step at N=2^20 (profiles/build_dram_N2p20.md)
-BUILD_DRAM_BYTES_PER_STEP = 687.0e6
+BUILD_DRAM_BYTES_PER_STEP = 469.5e6
 WORKLOAD = "cold-collapse uniform disc N=2^20, eps=0.005, theta=0.5, bucket=1, dt=5e-4, seed 7"
 
 def algorithmic_bytes(c: float) -> dict:
