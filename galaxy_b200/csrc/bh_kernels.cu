@@ -963,7 +963,7 @@ struct AggArgs {
     CellRec* groups;
 };
 
-// Aggregates of cell k (u = its record's (lo, skip, start, depth)): a leaf
+// Aggregates of cell k (u = its links (end, skip, start, depth)): a leaf
 // sums its bodies in Morton order, an internal cell its children in quadrant
 // order 0..3 (nbody/src/flat.rs:179-215).
 __device__ __forceinline__ void aggregate_cell(const AggArgs& a, uint32_t k, uint4 u, bool leaf) {
