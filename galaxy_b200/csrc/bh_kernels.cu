@@ -1056,7 +1056,7 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
         return left && right;
     };
     for (uint32_t k = kb + t; k < ke; k += kAggThreads) {
-        const uint4 u = a.cell_u[k];  // (0, skip, start, depth)
+        const uint4 u = a.cell_u[k];  // (end, skip, start, depth)
         const SimDesc& sd = a.sims[a.chunk_sim[u.z >> 5]];
         if (u.y == k + 1u) {
             aggregate_cell(a, k, u, true);
