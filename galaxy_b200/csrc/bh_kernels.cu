@@ -609,40 +609,41 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
     }
     uint32_t tile_total;
     const uint32_t texcl = block_exclusive_scan_256(sum, &tile_total, s_scan);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32u) {
+        // decoupled look-back by one warp: lane j reads tile tp - j, so a
+        // round covers 32 predecessors; a round counts once every tile up to
+        // the nearest inclusive prefix has published (tiles before 0 read as
+        // inclusive 0), otherwise it polls again (bounded)
+        const uint32_t lane = threadIdx.x;
         unsigned long long excl = 0;
         if (t == 0) {
-            atomicExch(&flags[0], kScanInc | (unsigned long long)tile_total);
+            if (lane == 0) atomicExch(&flags[0], kScanInc | (unsigned long long)tile_total);
         } else {
-            atomicExch(&flags[t], kScanAgg | (unsigned long long)tile_total);
-            uint32_t tp = t - 1;
+            if (lane == 0) atomicExch(&flags[t], kScanAgg | (unsigned long long)tile_total);
+            long long tp = (long long)t - 1;
             const long long c0 = clock64();
             while (true) {
-                unsigned long long f[kLookWindow];
+                const long long idx = tp - (long long)lane;
+                const unsigned long long f = idx >= 0 ? ld_volatile64(&flags[idx]) : kScanInc;
+                const unsigned long long st = f & ~kScanMask;
+                const uint32_t inc = __ballot_sync(kFull, st == kScanInc);
+                const uint32_t pub = __ballot_sync(kFull, st != 0ull);
+                const uint32_t upto = inc ? (inc & (0u - inc)) * 2u - 1u : 0xffffffffu;
+                if ((pub & upto) == upto) {
+                    unsigned long long v = ((upto >> lane) & 1u) ? (f & kScanMask) : 0ull;
 #pragma unroll
-                for (int j = 0; j < kLookWindow; ++j)
-                    f[j] = tp >= (uint32_t)j ? ld_volatile64(&flags[tp - j]) : 0ull;
-                bool done = false;
-                int used = 0;
-#pragma unroll
-                for (int j = 0; j < kLookWindow; ++j) {
-                    if (done || used < j) continue;
-                    const unsigned long long st = f[j] & ~kScanMask;
-                    if (st == 0ull) continue;
-                    excl += f[j] & kScanMask;
-                    used = j + 1;
-                    done = st == kScanInc;
-                }
-                if (done) break;
-                tp -= used;
-                if (used < kLookWindow && clock64() - c0 > kSpinCycles) {
-                    set_err(err, kErrLookbackTimeout);
-                    break;
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+                    excl += v;
+                    if (inc) break;
+                    tp -= 32;
+                } else if (__any_sync(kFull, clock64() - c0 > kSpinCycles)) {
+                    if (lane == 0) set_err(err, kErrLookbackTimeout);
+                    break;  // the whole warp: the vote is uniform
                 }
             }
-            atomicExch(&flags[t], kScanInc | (excl + tile_total));
+            if (lane == 0) atomicExch(&flags[t], kScanInc | (excl + tile_total));
         }
-        s_excl = excl;
+        if (lane == 0) s_excl = excl;
     }
     __syncthreads();
     uint32_t run = (uint32_t)s_excl + texcl;
