@@ -72,15 +72,17 @@ void release_state(std::unique_ptr<ServeRequest>& r) {
     r->st = nullptr;
 }
 
-int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active, bh_batch** b) {
+// Replaces *b by a batch of the active requests from index `from` on.
+int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active, bh_batch** b,
+               size_t from = 0) {
     if (*b) galaxy_bh_batch_destroy(*b);
     *b = nullptr;
-    if (active.empty()) return BH_OK;
+    if (active.size() <= from) return BH_OK;
     std::vector<bh_state*> states;
     std::vector<bh_config> cfgs;
-    for (auto& r : active) {
-        states.push_back(r->st);
-        cfgs.push_back(r->cfg);
+    for (size_t i = from; i < active.size(); ++i) {
+        states.push_back(active[i]->st);
+        cfgs.push_back(active[i]->cfg);
     }
     return galaxy_bh_batch_create(s->dev, states.data(), cfgs.data(), (uint32_t)states.size(), b);
 }
@@ -113,7 +115,9 @@ void serve_loop(bh_server* s) {
                 continue;
             }
         }
-        // admission, in arrival order, against the device-memory budget
+        // admission, in arrival order, against the device-memory budget;
+        // newcomers are appended after the members already stepping
+        const size_t stepping = active.size();
         bool joined = false;
         while (!waiting.empty() && active.size() < s->sc.max_members) {
             std::unique_ptr<ServeRequest>& cand = waiting.front();
@@ -150,10 +154,12 @@ void serve_loop(bh_server* s) {
         }
         if (active.empty()) continue;
         if (joined) {
-            // new members need their boundary acceleration; for members already
-            // stepping the solve reproduces theirs (same positions and tree)
-            int rc = form_batch(s, active, &batch);
+            // the newcomers need their boundary acceleration (a batch of them
+            // alone: members' results do not depend on their batch mates);
+            // the members already stepping hold theirs
+            int rc = form_batch(s, active, &batch, stepping);
             if (rc == BH_OK) rc = galaxy_bh_batch_solve(s->dev, batch);
+            if (rc == BH_OK) rc = form_batch(s, active, &batch);
             if (rc != BH_OK) {
                 fail_all_active(rc);
                 continue;
