@@ -422,8 +422,10 @@ __global__ void k_wait_probe(const uint32_t* flags, uint32_t* err, long long lim
 // lanes sharing a digit found with one ballot per digit bit), so equal
 // digits keep their input order: the permutation equals a stable sort by
 // code, as Rust's sort_by_key (nbody/src/flat.rs:233-234).
-template <int BITS, int PASS, bool LAST>
-__global__ void __launch_bounds__(kSortThreads) k_radix_pass(
+// MINB tiles share an SM: 2 (up to 128 registers) for sorts of one wave,
+// 3 (80 registers) for sorts of many waves of tiles (large batches).
+template <int BITS, int PASS, bool LAST, int MINB>
+__global__ void __launch_bounds__(kSortThreads, MINB) k_radix_pass(
     const SimDesc* __restrict__ sims, const Tile* __restrict__ tiles, uint32_t* tile_counter,
     const uint32_t* __restrict__ hist, uint32_t* flags, const uint32_t* __restrict__ keys_in,
     const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
@@ -1768,6 +1770,19 @@ cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s) {
 
 // Passes alternate a -> b -> a ...; an even pass count leaves the sorted keys
 // in keys_a / vals_a, and the last pass also gathers the sorted bodies.
+// Streaming multiprocessors of the current device (cached per device).
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
 template <int BITS, int PASS>
 static cudaError_t radix_passes(const BatchBuffers& b, cudaStream_t s) {
     constexpr int kPasses = 32 / BITS;
@@ -1777,10 +1792,17 @@ static cudaError_t radix_passes(const BatchBuffers& b, cudaStream_t s) {
     const uint32_t* vin = even ? b.vals_a : b.vals_b;
     uint32_t* kout = even ? b.keys_b : b.keys_a;
     uint32_t* vout = even ? b.vals_b : b.vals_a;
-    const cudaError_t e = launch_step(k_radix_pass<BITS, PASS, PASS == kPasses - 1>, b.ntiles,
-                                      kSortThreads, 0, s, b.sims, b.tiles, b.counters + PASS,
-                                      b.hist, b.sort_flags + PASS * fstride, kin,
-                                      PASS == 0 ? nullptr : vin, kout, vout, b.sbody, b.err);
+    // more than two waves of tiles at two per SM: three per SM instead
+    const bool many = b.ntiles > 2u * 2u * (uint32_t)sm_count();
+    const cudaError_t e =
+        many ? launch_step(k_radix_pass<BITS, PASS, PASS == kPasses - 1, 3>, b.ntiles,
+                           kSortThreads, 0, s, b.sims, b.tiles, b.counters + PASS, b.hist,
+                           b.sort_flags + PASS * fstride, kin, PASS == 0 ? nullptr : vin, kout,
+                           vout, b.sbody, b.err)
+             : launch_step(k_radix_pass<BITS, PASS, PASS == kPasses - 1, 2>, b.ntiles,
+                           kSortThreads, 0, s, b.sims, b.tiles, b.counters + PASS, b.hist,
+                           b.sort_flags + PASS * fstride, kin, PASS == 0 ? nullptr : vin, kout,
+                           vout, b.sbody, b.err);
     if (e != cudaSuccess) return e;
     if constexpr (PASS + 1 < kPasses) return radix_passes<BITS, PASS + 1>(b, s);
     return cudaSuccess;
