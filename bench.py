@@ -874,11 +874,14 @@ def run_large_roofline(gpu, rt, peak_gbs: float, n: int = 1 << 24, reps: int = 3
     tree = rt.create_tree(gpu, ev, cfg)
     rt.rebuild(gpu, ev, tree, cfg)
     stage = {"integrate": 0.0, "morton": 0.0, "radix": 0.0, "topology": 0.0, "aggregate": 0.0}
+    import torch
+    torch.cuda.nvtx.range_push("n2p24")  # ncu --nvtx --nvtx-include n2p24/
     for _ in range(reps):
         stage["integrate"] += gpu.kick_drift(ev, DT).dispatch_seconds / reps
         bt = rt.rebuild(gpu, ev, tree, cfg)
         for k in ("morton", "radix", "topology", "aggregate"):
             stage[k] += getattr(bt, k + "_seconds") / reps
+    torch.cuda.nvtx.range_pop()
     c = tree_cells(gpu, rt, tree) / n
     tree.close()
     ev.close()
