@@ -78,12 +78,18 @@ struct bh_device {
     // freeing and allocating gigabytes each time.
     void* spare = nullptr;
     size_t spare_bytes = 0;
+    // Stream-ordered pool of the per-state buffers.  It keeps released
+    // memory for the next state (trimmed only when an arena allocation runs
+    // short): cudaFree synchronizes the device and unmaps pages, which cost
+    // a serving loop seconds per burst of finished requests.
+    cudaMemPool_t pool = nullptr;
 };
 
 static void device_free(bh_device* dev) {
     cudaSetDevice(dev->ordinal);
     cudaStreamSynchronize(dev->stream);
     cudaFree(dev->spare);
+    if (dev->pool) cudaMemPoolDestroy(dev->pool);
     for (auto& ev : dev->ev) cudaEventDestroy(ev);
     cudaStreamDestroy(dev->stream);
     delete dev;
@@ -119,9 +125,19 @@ extern "C" int galaxy_bh_device_open(int ordinal, bh_device** out) {
                          count - 1);
     bh_device* d = new bh_device();
     d->ordinal = ordinal;
+    cudaMemPoolProps pool_props{};
+    pool_props.allocType = cudaMemAllocationTypePinned;
+    pool_props.location.type = cudaMemLocationTypeDevice;
+    pool_props.location.id = ordinal;
+    const uint64_t keep = ~0ull;
     if ((e = cudaSetDevice(ordinal)) != cudaSuccess ||
         (e = cudaGetDeviceProperties(&d->prop, ordinal)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        (e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaMemPoolCreate(&d->pool, &pool_props)) != cudaSuccess ||
+        (e = cudaMemPoolSetAttribute(d->pool, cudaMemPoolAttrReleaseThreshold,
+                                     (void*)&keep)) != cudaSuccess) {
+        if (d->pool) cudaMemPoolDestroy(d->pool);
+        if (d->stream) cudaStreamDestroy(d->stream);
         delete d;
         return cuda_fail(e, "device open");
     }
@@ -255,11 +271,14 @@ extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host
     cudaEventRecord(dev->ev[0], dev->stream);
     cudaError_t e;
     std::vector<uint32_t> chunk(st->nchunks, 0u);
-    if ((e = cudaMalloc(&st->d_state, sizeof(GpuEvolveState) * (size_t)n)) ||
-        (e = cudaMalloc(&st->d_accel, sizeof(float4) * (size_t)n)) ||
-        (e = cudaMalloc(&st->d_sim, sizeof(SimDesc))) ||
-        (e = cudaMalloc(&st->d_chunk_sim, sizeof(uint32_t) * st->nchunks)) ||
-        (e = cudaMalloc(&st->d_minmax, 16)) || (e = cudaMalloc(&st->d_check, 16))) {
+    auto pool_alloc = [&](auto** ptr, size_t bytes) {
+        return cudaMallocFromPoolAsync((void**)ptr, bytes, dev->pool, dev->stream);
+    };
+    if ((e = pool_alloc(&st->d_state, sizeof(GpuEvolveState) * (size_t)n)) ||
+        (e = pool_alloc(&st->d_accel, sizeof(float4) * (size_t)n)) ||
+        (e = pool_alloc(&st->d_sim, sizeof(SimDesc))) ||
+        (e = pool_alloc(&st->d_chunk_sim, sizeof(uint32_t) * st->nchunks)) ||
+        (e = pool_alloc(&st->d_minmax, 16)) || (e = pool_alloc(&st->d_check, 16))) {
         galaxy_bh_state_destroy(st);
         return cuda_fail(e, "evolving state allocation");
     }
@@ -296,15 +315,13 @@ extern "C" int galaxy_bh_state_destroy(bh_state* st) {
     if (st->dev) {
         cudaSetDevice(st->dev->ordinal);
         cudaStreamSynchronize(st->dev->stream);
+        // back to the device's pool, in stream order (no device-wide sync)
+        for (void* p : {(void*)st->d_state, (void*)st->d_accel, (void*)st->d_sim,
+                        (void*)st->d_chunk_sim, (void*)st->d_minmax, (void*)st->d_check})
+            if (p) cudaFreeAsync(p, st->dev->stream);
     }
-    cudaFree(st->d_state);
-    cudaFree(st->d_accel);
     cudaFree(st->d_potential);
-    cudaFree(st->d_sim);
-    cudaFree(st->d_chunk_sim);
-    cudaFree(st->d_minmax);
     cudaFree(st->d_cons);
-    cudaFree(st->d_check);
     cudaFree(st->d_stage);
     bh_device* dev = st->dev;
     delete st;
@@ -680,6 +697,13 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
         dev->spare = nullptr;
         dev->spare_bytes = 0;
         e = cudaMalloc(&b->arena, b->arena_bytes);
+        if (e == cudaErrorMemoryAllocation) {
+            // give back the released state memory the pool keeps, then retry
+            cudaGetLastError();
+            cudaStreamSynchronize(dev->stream);
+            cudaMemPoolTrimTo(dev->pool, 0);
+            e = cudaMalloc(&b->arena, b->arena_bytes);
+        }
         b->arena_capacity = b->arena_bytes;
     }
     if (e != cudaSuccess) {

@@ -259,23 +259,28 @@ extern "C" int galaxy_bh_serve_submit(bh_server* s, const GpuEvolveState* host, 
 extern "C" int galaxy_bh_serve_poll(bh_server* s, uint32_t timeout_ms, bh_serve_result* res,
                                     GpuEvolveState* out, uint32_t capacity) {
     if (!s || !res) return set_error_message(BH_INVALID_ARG, "null argument");
-    std::unique_lock<std::mutex> lk(s->mu);
-    if (!s->cv_out.wait_for(lk, std::chrono::milliseconds(timeout_ms),
-                            [&] { return !s->done.empty(); }))
-        return set_error_message(BH_TIMEOUT, "no finished request within the timeout");
-    ServeRequest& r = *s->done.front();
-    res->request_id = r.id;
-    res->n = r.n;
-    if (r.status == BH_OK && (!out || capacity < r.n))  // kept for a retry with room
-        return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
-    res->n = r.n;
+    std::unique_ptr<ServeRequest> taken;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (!s->cv_out.wait_for(lk, std::chrono::milliseconds(timeout_ms),
+                                [&] { return !s->done.empty(); }))
+            return set_error_message(BH_TIMEOUT, "no finished request within the timeout");
+        const ServeRequest& r = *s->done.front();
+        res->request_id = r.id;
+        res->n = r.n;
+        if (r.status == BH_OK && (!out || capacity < r.n))  // kept for a retry with room
+            return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
+        taken = std::move(s->done.front());
+        s->done.pop_front();
+    }
+    // the copy and the release of the records run without the server's lock
+    const ServeRequest& r = *taken;
     res->status = (uint32_t)r.status;
     res->steps = r.steps;
     res->submitted_s = r.submitted_s;
     res->admitted_s = r.admitted_s;
     res->finished_s = r.finished_s;
     if (r.status == BH_OK) std::memcpy(out, r.records.data(), sizeof(GpuEvolveState) * r.n);
-    s->done.pop_front();
     return BH_OK;
 }
 
