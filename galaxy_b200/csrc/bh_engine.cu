@@ -241,16 +241,8 @@ struct bh_state {
     SimDesc h_sim{};
 };
 
-static int check_state_records(const GpuEvolveState* h, uint32_t n) {
-    for (uint32_t i = 0; i < n; ++i) {
-        const GpuEvolveState& s = h[i];
-        if (!std::isfinite(s.position_mass[0]) || !std::isfinite(s.position_mass[1]) ||
-            !std::isfinite(s.velocity[0]) || !std::isfinite(s.velocity[1]) ||
-            !std::isfinite(s.position_mass[2]) || !(s.position_mass[2] > 0.f))
-            return set_error(BH_NONFINITE, "body %u contains invalid evolving state", i);
-    }
-    return BH_OK;
-}
+static int enqueue_check(bh_state* st, const void* records, int kind, uint32_t n);
+static int fetch_check(bh_state* st, uint32_t* first_bad);
 
 extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host, uint32_t n,
                                       bh_state** out, bh_stage_timing* timing) {
@@ -262,7 +254,6 @@ extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host
     if (n < 2 || n > (1u << 30))
         return set_error(BH_INVALID_ARG, "GPU evolving state requires 2..=%u resident bodies",
                          1u << 30);
-    if ((rc = check_state_records(host, n))) return rc;
     bh_state* st = new bh_state();
     st->dev = dev;
     device_ref(dev);
@@ -297,9 +288,17 @@ extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host
         return cuda_fail(e, "evolving state upload");
     }
     cudaEventRecord(dev->ev[1], dev->stream);
-    if ((e = cudaStreamSynchronize(dev->stream))) {
+    // nbody_gpu.rs:802-810: every record finite with a positive mass, tested
+    // on the uploaded copy; the smallest failing index is reported and no
+    // state is created
+    uint32_t bad = kNone;
+    if ((rc = enqueue_check(st, st->d_state, 0, n)) || (rc = fetch_check(st, &bad))) {
         galaxy_bh_state_destroy(st);
-        return cuda_fail(e, "evolving state upload");
+        return rc;
+    }
+    if (bad != kNone) {
+        galaxy_bh_state_destroy(st);
+        return set_error(BH_NONFINITE, "body %u contains invalid evolving state", bad);
     }
     if (timing) {
         float ms = 0.f;

@@ -398,6 +398,37 @@ def test_state_upload_and_readback_checks(gpu, oracle):
     assert np.array_equal(out.view(np.float32).reshape(-1, 8), want)
 
 
+def test_state_create_rejects_invalid_records(gpu):
+    """state_create tests every uploaded record (finite position, velocity
+    and mass, mass > 0: nbody_gpu.rs:802-810), reports the smallest failing
+    index and creates no state; valid records upload bit for bit."""
+    import ctypes as C
+
+    from galaxy_b200 import _lib
+    L = _lib.load()
+    recs = np.zeros(5000, _lib.EVOLVE_STATE_DTYPE)
+    f = recs.view(np.float32).reshape(-1, 8)
+    f[:, 0] = np.linspace(-1.0, 1.0, len(f), dtype=np.float32)
+    f[:, 1] = np.float32(0.5)
+    f[:, 2] = np.float32(1e-3)
+    for idx, col, val in ((4321, 2, -1.0), (77, 5, np.inf), (4999, 0, np.nan)):
+        bad = recs.copy()
+        bad.view(np.float32).reshape(-1, 8)[idx, col] = val
+        if idx + 1 < len(bad):
+            bad.view(np.float32).reshape(-1, 8)[-1, 2] = 0.0  # a later failure too
+        st = C.c_void_p()
+        rc = L.galaxy_bh_state_create(gpu.handle, _lib.ptr(bad), len(bad), C.byref(st), None)
+        assert rc == _lib.BH_NONFINITE
+        assert f"body {idx} " in _lib.last_error()
+        assert not st.value
+    st = C.c_void_p()
+    _lib.check(L.galaxy_bh_state_create(gpu.handle, _lib.ptr(recs), len(recs), C.byref(st), None))
+    out = np.zeros_like(recs)
+    _lib.check(L.galaxy_bh_read_state(gpu.handle, st, _lib.ptr(out), len(out), None))
+    assert np.array_equal(out.view(np.uint32), recs.view(np.uint32))
+    _lib.check(L.galaxy_bh_state_destroy(st))
+
+
 def test_force_after_step_reproduces_step_accelerations(gpu, rt):
     """A force on the tree a step left behind (same positions) recomputes the
     step's closing accelerations bit for bit, with or without the potential
