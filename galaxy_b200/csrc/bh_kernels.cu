@@ -1292,36 +1292,27 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
         const uint32_t ha = max(u.y, p0), hb = min(u.y + u.z, p0 + 32u);
         const uint32_t H = (present && ha < hb) ? bit_range(ha - p0, hb - p0) : 0u;
         const uint32_t R = A & ~H;
-        uint32_t ap = 0u, op = 0u;
-        bool mixed = false, multi = false;
-        if (present) {
-            if (leaf) {
-                if (u.z == 1u)
-                    ap = R;
-                else
-                    multi = true;
-            } else {
-                op = A & H;
-                if (R) {
-                    const float nx = fmaxf(fmaxf(bx0 - f.x, f.x - bx1), 0.f);
-                    const float ny = fmaxf(fmaxf(by0 - f.y, f.y - by1), 0.f);
-                    const float fx = fmaxf(fabsf(f.x - bx0), fabsf(f.x - bx1));
-                    const float fy = fmaxf(fabsf(f.y - by0), fabsf(f.y - by1));
-                    if (dist2(nx, ny) > f.w)
-                        ap = R;
-                    else if (dist2(fx, fy) < __uint_as_float(u.x))
-                        op |= R;
-                    else
-                        mixed = true;
-                }
-            }
-            if (STATS) {
-                n_visit += __popc(A);
-                if (leaf)
-                    n_direct += __popc(ap);
-                else
-                    n_approx += __popc(ap);
-            }
+        // classification, branch-free (a select per outcome): a one-body
+        // leaf is a list term for R; an internal cell is a list term for R
+        // when the box's nearest point is beyond hi, opened by R when its
+        // farthest corner is inside lo, otherwise mixed; holding lanes open it
+        const float nx = fmaxf(fmaxf(bx0 - f.x, f.x - bx1), 0.f);
+        const float ny = fmaxf(fmaxf(by0 - f.y, f.y - by1), 0.f);
+        const float fx = fmaxf(fabsf(f.x - bx0), fabsf(f.x - bx1));
+        const float fy = fmaxf(fabsf(f.y - by0), fabsf(f.y - by1));
+        const bool internal = present && !leaf;
+        const bool far = dist2(nx, ny) > f.w;
+        const bool near = dist2(fx, fy) < __uint_as_float(u.x);
+        const bool multi = present && leaf && u.z != 1u;
+        const uint32_t ap = ((present && leaf && u.z == 1u) || (internal && far)) ? R : 0u;
+        uint32_t op = internal ? ((A & H) | ((!far && near) ? R : 0u)) : 0u;
+        const bool mixed = internal && R != 0u && !far && !near;
+        if (STATS && present) {
+            n_visit += __popc(A);
+            if (leaf)
+                n_direct += __popc(ap);
+            else
+                n_approx += __popc(ap);
         }
         if (STATS) ++n_iter;
 
@@ -1355,10 +1346,9 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
                     if (STATS) ++n_exact;
                 }
             }
-            if (__any_sync(kFull, approx)) {
-                term(dx, dy, d2, cf.z, approx);
-                if (STATS) n_approx += approx;
-            }
+            // branch-free: lanes that do not approximate add a zero term
+            term(dx, dy, d2, cf.z, approx);
+            if (STATS) n_approx += approx;
             const uint32_t O = __ballot_sync(kFull, open);
             if (lane == 0) s_mix[warp][i].w = O;
             if (STATS) ++n_iter;
