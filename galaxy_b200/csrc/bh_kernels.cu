@@ -1260,10 +1260,17 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
             const float4 e = list[i];
             const float dx = e.x - tx, dy = e.y - ty;
             const float inv_r = rsqrtf(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, eps2)));
-            const float gm = (__float_as_uint(e.w) & lane_bit) ? e.z : 0.f;
-            const float scale = gm * inv_r * inv_r * inv_r;
-            acc.add(dx * scale, dy * scale);
-            if (POT) phi -= gm * inv_r;
+            const bool take = (__float_as_uint(e.w) & lane_bit) != 0u;
+            if constexpr (!COMP && !POT) {
+                // plain sums: lanes outside the mask skip the (predicated) adds
+                const float scale = e.z * inv_r * inv_r * inv_r;
+                if (take) acc.add(dx * scale, dy * scale);
+            } else {
+                const float gm = take ? e.z : 0.f;
+                const float scale = gm * inv_r * inv_r * inv_r;
+                acc.add(dx * scale, dy * scale);
+                if (POT) phi -= gm * inv_r;
+            }
         }
     };
 
