@@ -151,7 +151,10 @@ int galaxy_bh_device_stream(bh_device* dev, void** stream);
 /* ---- persistent evolving state -------------------------------------------
  * Replaces NbodyGpu::create_evolving_state (nbody_gpu.rs:786-852).  host
  * holds n GpuEvolveState records (the host side does the f64->f32
- * checked_f32 conversion).  Requires 2 <= n, finite values and mass > 0. */
+ * checked_f32 conversion).  Requires 2 <= n, finite values and mass > 0,
+ * tested on the uploaded copy: BH_NONFINITE names the smallest failing index
+ * and no state is created.  The state's buffers come from a stream-ordered
+ * pool of the device handle, released in order on its stream. */
 int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host, uint32_t n,
                            bh_state** out, bh_stage_timing* timing);
 int galaxy_bh_state_destroy(bh_state* st);
