@@ -132,6 +132,8 @@ SIGNATURES = {
                                          C.POINTER(BhBuildTiming)]),
     "galaxy_bh_force": (C.c_int, [_P, _P, _P, C.POINTER(BhConfig), C.POINTER(BhStageTiming)]),
     "galaxy_bh_force_stats": (C.c_int, [_P, _P, C.POINTER(BhForceStats)]),
+    "galaxy_bh_force_f64": (C.c_int, [_P, _P, _P, C.POINTER(BhConfig), _P, _P,
+                                      C.POINTER(BhForceStats)]),
     "galaxy_bh_wait_probe": (C.c_int, [_P, C.c_uint64]),
     "galaxy_bh_read_tree_evidence": (C.c_int, [_P, _P, _P, _P, _P, _U32, _P, _U32,
                                                C.POINTER(_U32)]),

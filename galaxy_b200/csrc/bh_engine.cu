@@ -1051,6 +1051,42 @@ extern "C" int galaxy_bh_force_stats(bh_device* dev, bh_tree* tree, bh_force_sta
     return BH_OK;
 }
 
+extern "C" int galaxy_bh_force_f64(bh_device* dev, bh_state* st, bh_tree* tree,
+                                   const bh_config* cfg, double* accel, double* abs_sum,
+                                   bh_force_stats* stats) {
+    int rc = tree_check(dev, st, tree);
+    if (rc) return rc;
+    if (!cfg || !accel) return set_error(BH_INVALID_ARG, "null argument");
+    if ((rc = validate_config(cfg))) return rc;
+    if (!tree->built) return set_error(BH_INVALID_ARG, "force requires a rebuilt tree");
+    const size_t n = st->n;
+    const size_t bytes = 16 * n + (abs_sum ? 8 * n : 0) + 32;
+    char* d = nullptr;
+    CK(cudaMalloc(&d, bytes), "f64 traversal allocation");
+    double* d_acc = reinterpret_cast<double*>(d);
+    double* d_abs = abs_sum ? reinterpret_cast<double*>(d + 16 * n) : nullptr;
+    unsigned long long* d_stats = reinterpret_cast<unsigned long long*>(d + bytes - 32);
+    unsigned long long h_stats[3] = {0, 0, 0};
+    cudaError_t e = cudaMemsetAsync(d_stats, 0, 32, dev->stream);
+    if (!e)
+        e = launch_traverse_f64(tree->batch->bb, 0, st->n, cfg->theta, cfg->softening, cfg->g,
+                                d_acc, d_abs, d_stats, dev->stream);
+    if (!e) e = cudaMemcpyAsync(accel, d_acc, 16 * n, cudaMemcpyDeviceToHost, dev->stream);
+    if (!e && abs_sum)
+        e = cudaMemcpyAsync(abs_sum, d_abs, 8 * n, cudaMemcpyDeviceToHost, dev->stream);
+    if (!e) e = cudaMemcpyAsync(h_stats, d_stats, 24, cudaMemcpyDeviceToHost, dev->stream);
+    if (!e) e = cudaStreamSynchronize(dev->stream);
+    cudaFree(d);
+    if (e) return cuda_fail(e, "f64 traversal");
+    if (stats) {
+        *stats = bh_force_stats{};
+        stats->visited_nodes = h_stats[0];
+        stats->approximated_cells = h_stats[1];
+        stats->direct_terms = h_stats[2];
+    }
+    return BH_OK;
+}
+
 extern "C" int galaxy_bh_wait_probe(bh_device* dev, uint64_t spin_cycles) {
     int rc = enter(dev);
     if (rc) return rc;

@@ -107,7 +107,8 @@ struct BatchBuffers {
                         // refresh); the MAC fields live in the node-group slots
     CellRec* groups;    // node groups: children of cell k at [4k, 4k+4); simulation s's
                         // root at slot 0 of group cell_capacity + s (traversal)
-    double4* cell_d;    // com_x, com_y, mass, 0 (f64)
+    double4* cell_d;    // com_x, com_y, mass (f64), then the f32 residuals of
+                        // com_x, com_y (float2 bits): com - (float)com
     uint4* cell_child;  // children (global cell indices)
     uint32_t* cell_parent;
     uint32_t* cell_counter;
@@ -144,6 +145,13 @@ cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bo
 cudaError_t launch_direct_probes(const GpuEvolveState* state, uint32_t n, const uint32_t* probes,
                                  uint32_t nprobes, double eps, double g, double* out,
                                  cudaStream_t s);
+// The reference's f64 flat traversal over the tree of simulation `sim` (n
+// bodies): out gets (ax, ay) per body in resident order, abs_sum (or null)
+// the sum of term magnitudes, stats (or null, 3 counters, pre-zeroed) the
+// visited / approximated / direct counts.
+cudaError_t launch_traverse_f64(const BatchBuffers& b, uint32_t sim, uint32_t n, double theta,
+                                double eps, double g, double* out, double* abs_sum,
+                                unsigned long long* stats, cudaStream_t s);
 // FP64 conservation partial sums: out gets 9 doubles (see galaxy_bh_conservation).
 cudaError_t launch_conservation(const GpuEvolveState* state, const float* potential, uint32_t n,
                                 double* partials, uint32_t nblocks, double* out,

@@ -200,6 +200,8 @@ constexpr long long kSpinCycles = 2000000000ll;
 // final kick of one step and the kick-drift of the next with the same two
 // roundings as two separate launches.  Modes 0, 1, 3 also reduce the
 // per-simulation f32 bounds of the (new) positions.
+constexpr int kIntegrateUnroll = 4;  // chunks whose loads a warp keeps in flight
+
 template <int MODE>
 __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ sims,
                                                    const uint32_t* __restrict__ chunk_sim,
@@ -209,8 +211,17 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
     __shared__ uint32_t s_sim[8];
     __shared__ float s_val[8][4];
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    // each warp streams a contiguous run of chunks
     const uint32_t nwarps = gridDim.x * 8;
+    const uint32_t per = (nchunks + nwarps - 1) / nwarps;
+    const uint32_t c_begin = min((blockIdx.x * 8 + warp) * per, nchunks);
+    const uint32_t c_end = min(c_begin + per, nchunks);
     uint32_t cur = kNone;
+    // fields of simulation `cur`, reloaded only when the simulation changes
+    GpuEvolveState* st = nullptr;
+    const float4* acc = nullptr;
+    uint32_t off = 0, n = 0;
+    float dt = 0.f;
     float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
 
     auto warp_reduce = [&]() {
@@ -222,53 +233,109 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
             mxy = fmaxf(mxy, __shfl_xor_sync(kFull, mxy, o));
         }
     };
-
-    for (uint32_t chunk = blockIdx.x * 8 + warp; chunk < nchunks; chunk += nwarps) {
-        const uint32_t s = chunk_sim[chunk];
-        if (s == kNone) continue;
-        if (kBounds && s != cur) {
-            if (cur != kNone) {
-                warp_reduce();
-                if (lane == 0) {
-                    atomicMax(&minmax[4 * cur + 0], ~enc_f32(mnx));
-                    atomicMax(&minmax[4 * cur + 1], ~enc_f32(mny));
-                    atomicMax(&minmax[4 * cur + 2], enc_f32(mxx));
-                    atomicMax(&minmax[4 * cur + 3], enc_f32(mxy));
-                }
-                mnx = mny = INFINITY;
-                mxx = mxy = -INFINITY;
+    // warp-uniform: publishes the bounds of the previous simulation
+    auto enter_sim = [&](uint32_t s) {
+        if (s == cur) return;
+        if (kBounds && cur != kNone) {
+            warp_reduce();
+            if (lane == 0) {
+                atomicMax(&minmax[4 * cur + 0], ~enc_f32(mnx));
+                atomicMax(&minmax[4 * cur + 1], ~enc_f32(mny));
+                atomicMax(&minmax[4 * cur + 2], enc_f32(mxx));
+                atomicMax(&minmax[4 * cur + 3], enc_f32(mxy));
             }
-            cur = s;
+            mnx = mny = INFINITY;
+            mxx = mxy = -INFINITY;
         }
+        cur = s;
         const SimDesc& sd = sims[s];
-        const uint32_t i = chunk * kChunk + lane - sd.off;
-        if (i < sd.n) {
-            float4* rec = reinterpret_cast<float4*>(sd.state + i);
-            float4 pm = rec[0];
+        st = sd.state;
+        acc = sd.accel;
+        off = sd.off;
+        n = sd.n;
+        dt = sd.dt;
+    };
+    // the kick / drift of one record, with its bounds
+    auto update = [&](float4& pm, float4& v, const float4& a) {
+        const float hdt = __fmul_rn(0.5f, dt);
+        if (MODE == 2 || MODE == 3) {
+            v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
+            v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
+        }
+        if (MODE == 1 || MODE == 3) {
+            v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
+            v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
+            pm.x = __fadd_rn(pm.x, __fmul_rn(dt, v.x));
+            pm.y = __fadd_rn(pm.y, __fmul_rn(dt, v.y));
+        }
+    };
+    auto bound = [&](const float4& pm) {
+        if (kBounds) {
+            mnx = fminf(mnx, pm.x);
+            mny = fminf(mny, pm.y);
+            mxx = fmaxf(mxx, pm.x);
+            mxy = fmaxf(mxy, pm.y);
+        }
+    };
+    auto one_chunk = [&](uint32_t chunk, uint32_t s) {
+        if (s == kNone) return;
+        enter_sim(s);
+        const uint32_t i = chunk * kChunk + lane - off;
+        if (i >= n) return;
+        float4* rec = reinterpret_cast<float4*>(st + i);
+        float4 pm = rec[0];
+        if (MODE != 0) {
+            float4 v = rec[1];
+            update(pm, v, acc[i]);
+            if (MODE != 2) rec[0] = pm;
+            rec[1] = v;
+        }
+        bound(pm);
+    };
+
+    constexpr uint32_t kPast = kNone - 1u;  // a slot past the warp's last chunk
+    for (uint32_t chunk = c_begin; chunk < c_end; chunk += kIntegrateUnroll) {
+        uint32_t sv[kIntegrateUnroll];
+#pragma unroll
+        for (int j = 0; j < kIntegrateUnroll; ++j)
+            sv[j] = chunk + j < c_end ? chunk_sim[chunk + j] : kPast;
+        bool same = sv[0] != kNone;
+#pragma unroll
+        for (int j = 1; j < kIntegrateUnroll; ++j) same = same && (sv[j] == sv[0] || sv[j] == kPast);
+        if (!same) {
+#pragma unroll 1
+            for (int j = 0; j < kIntegrateUnroll; ++j)
+                if (sv[j] != kPast) one_chunk(chunk + j, sv[j]);
+            continue;
+        }
+        // one simulation: every load of the run first, then the updates
+        enter_sim(sv[0]);
+        float4 pm[kIntegrateUnroll], v[kIntegrateUnroll], a[kIntegrateUnroll];
+        bool ok[kIntegrateUnroll];
+#pragma unroll
+        for (int j = 0; j < kIntegrateUnroll; ++j) {
+            const uint32_t i = (chunk + j) * kChunk + lane - off;
+            ok[j] = sv[j] != kPast && i < n;
+            if (ok[j]) {
+                const float4* rec = reinterpret_cast<const float4*>(st + i);
+                pm[j] = rec[0];
+                if (MODE != 0) {
+                    v[j] = rec[1];
+                    a[j] = acc[i];
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kIntegrateUnroll; ++j) {
+            if (!ok[j]) continue;
+            const uint32_t i = (chunk + j) * kChunk + lane - off;
             if (MODE != 0) {
-                float4 v = rec[1];
-                const float4 a = sd.accel[i];
-                const float dt = sd.dt;
-                const float hdt = __fmul_rn(0.5f, dt);
-                if (MODE == 2 || MODE == 3) {
-                    v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
-                    v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
-                }
-                if (MODE == 1 || MODE == 3) {
-                    v.x = __fadd_rn(v.x, __fmul_rn(hdt, a.x));
-                    v.y = __fadd_rn(v.y, __fmul_rn(hdt, a.y));
-                    pm.x = __fadd_rn(pm.x, __fmul_rn(dt, v.x));
-                    pm.y = __fadd_rn(pm.y, __fmul_rn(dt, v.y));
-                    rec[0] = pm;
-                }
-                rec[1] = v;
+                update(pm[j], v[j], a[j]);
+                float4* rec = reinterpret_cast<float4*>(st + i);
+                if (MODE != 2) rec[0] = pm[j];
+                rec[1] = v[j];
             }
-            if (kBounds) {
-                mnx = fminf(mnx, pm.x);
-                mny = fminf(mny, pm.y);
-                mxx = fmaxf(mxx, pm.x);
-                mxy = fmaxf(mxy, pm.y);
-            }
+            bound(pm[j]);
         }
     }
     if (!kBounds) return;
@@ -922,8 +989,14 @@ __device__ __forceinline__ void store_cell_values(uint32_t k, double mass, doubl
                                                   double4* cell_d, CellRec* groups) {
     const double com_x = __ddiv_rn(wx, mass);
     const double com_y = __ddiv_rn(wy, mass);
-    cell_d[k] = make_double4(com_x, com_y, mass, 0.0);
-    store_mac_fields(groups, k, (float)com_x, (float)com_y, __fmul_rn(g, (float)mass),
+    const float hx = (float)com_x, hy = (float)com_y;
+    // the f32 residuals com - (float)com ride in the record's spare word: the
+    // compensated traversal adds them back to its differences
+    const float lo_x = (float)(com_x - (double)hx), lo_y = (float)(com_y - (double)hy);
+    const unsigned long long lo_bits =
+        ((unsigned long long)__float_as_uint(lo_y) << 32) | __float_as_uint(lo_x);
+    cell_d[k] = make_double4(com_x, com_y, mass, __longlong_as_double((long long)lo_bits));
+    store_mac_fields(groups, k, hx, hy, __fmul_rn(g, (float)mass),
                      depth, start, count, leaf, slot, root_half, theta);
 }
 
@@ -1212,6 +1285,11 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
     __shared__ float4 s_list[WARPS][kTravList];   // (com_x, com_y, G*m, lane mask bits)
     __shared__ uint4 s_mix[WARPS][32];  // mixed cells by rank: (lo bits, cell, deciding
                                         // lanes, opened); their f in list[32 + rank]
+    // compensated form: the f32 residual of each list entry's centre of mass
+    // (0 for bodies), added back to the difference (com_hi - x) + com_lo, so a
+    // term's distance carries the f64 centre of mass to one f32 rounding of
+    // the distance itself rather than of the centre's coordinates
+    __shared__ float2 s_lo[WARPS][COMP ? kTravList : 1];
     const uint32_t lane = lane_id();
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t chunk = blockIdx.x * WARPS + warp;
@@ -1258,7 +1336,12 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
 #pragma unroll 4
         for (uint32_t i = 0; i < count; ++i) {
             const float4 e = list[i];
-            const float dx = e.x - tx, dy = e.y - ty;
+            float dx = e.x - tx, dy = e.y - ty;
+            if constexpr (COMP) {
+                const float2 lo = s_lo[warp][i];
+                dx += lo.x;
+                dy += lo.y;
+            }
             const float inv_r = rsqrtf(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, eps2)));
             const bool take = (__float_as_uint(e.w) & lane_bit) != 0u;
             if constexpr (!COMP && !POT) {
@@ -1295,6 +1378,12 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
         const uint32_t A = e.y;
         const bool present = u.z != 0u;
         const bool leaf = u.w == kNone;
+        float2 clo = make_float2(0.f, 0.f);  // compensated: residual of the centre of mass
+        if (COMP && have && present && !leaf) {
+            const unsigned long long b = __double_as_longlong(
+                __ldg(reinterpret_cast<const double*>(cell_d + u.w) + 3));
+            clo = make_float2(__uint_as_float((uint32_t)b), __uint_as_float((uint32_t)(b >> 32)));
+        }
         // lanes whose own body the cell holds: positions [start, start + count)
         const uint32_t ha = max(u.y, p0), hb = min(u.y + u.z, p0 + 32u);
         const uint32_t H = (present && ha < hb) ? bit_range(ha - p0, hb - p0) : 0u;
@@ -1332,6 +1421,7 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
         const uint32_t mrank = __popc(bm & lanes_below);
         if (mixed) {
             list[32u + mrank] = f;
+            if (COMP) s_lo[warp][32u + mrank] = clo;
             s_mix[warp][mrank] = make_uint4(u.x, u.w, R, 0u);
         }
         __syncwarp();
@@ -1354,7 +1444,13 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
                 }
             }
             // branch-free: lanes that do not approximate add a zero term
-            term(dx, dy, d2, cf.z, approx);
+            if constexpr (COMP) {
+                const float2 lo = s_lo[warp][32u + i];
+                const float cx = dx + lo.x, cy = dy + lo.y;
+                term(cx, cy, dist2(cx, cy), cf.z, approx);
+            } else {
+                term(dx, dy, d2, cf.z, approx);
+            }
             if (STATS) n_approx += approx;
             const uint32_t O = __ballot_sync(kFull, open);
             if (lane == 0) s_mix[warp][i].w = O;
@@ -1383,7 +1479,11 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
 
         // append the uniform terms, push the opened groups in lane order
         const uint32_t la = __ballot_sync(kFull, ap != 0u);
-        if (ap) list[nlist + __popc(la & lanes_below)] = make_float4(f.x, f.y, f.z, __uint_as_float(ap));
+        if (ap) {
+            const uint32_t slot = nlist + __popc(la & lanes_below);
+            list[slot] = make_float4(f.x, f.y, f.z, __uint_as_float(ap));
+            if (COMP) s_lo[warp][slot] = clo;
+        }
         nlist += __popc(la);
         const uint32_t lp = __ballot_sync(kFull, op != 0u);
         if (len + __popc(lp) > kTravStack) {  // unreachable by the bound above
@@ -1692,6 +1792,107 @@ cudaError_t launch_direct_probes(const GpuEvolveState* state, uint32_t n, const 
     return cudaGetLastError();
 }
 
+// ================================================= f64 flat traversal =====
+
+// The reference CPU flat traversal (flat_acceleration_for,
+// nbody/src/flat.rs:270-346) in f64 over this engine's tree, one thread per
+// body in Morton order.  The cells are numbered in the reference's preorder,
+// so its depth-first stack walk (children pushed 3..0, popped 0 first) is
+// the walk k -> k + 1 when a cell opens and k -> skip when a leaf is summed
+// or a cell approximated: each body meets the same cells in the same order,
+// with the same f64 centres of mass and masses (bit-identical aggregates),
+// the same MAC (hypot distance, width / distance < theta, a cell holding the
+// body always opens) and the per-term arithmetic of nbody/src/lib.rs:247-255
+// as explicit round-to-nearest operations, so the sum repeats the
+// reference's additions one for one.  abs_sum (optional) gets the sum of
+// the terms' magnitudes |G m d / r^3| per body; stats the reference's force
+// counters (visited, approximated, direct).
+constexpr int kF64Threads = 128;
+
+__global__ void __launch_bounds__(kF64Threads) k_traverse_f64(
+    const SimDesc* __restrict__ sims, const SimOut* __restrict__ simout, uint32_t sim,
+    const float4* __restrict__ sbody, const uint4* __restrict__ cell_u,
+    const double4* __restrict__ cell_d, const uint32_t* __restrict__ base, double theta,
+    double eps, double g, double2* __restrict__ out, double* __restrict__ abs_sum,
+    unsigned long long* __restrict__ stats) {
+    const SimDesc& sd = sims[sim];
+    const uint32_t i = blockIdx.x * kF64Threads + threadIdx.x;
+    unsigned long long nv = 0, na = 0, nd = 0;
+    if (i < sd.n) {
+        const uint32_t p = sd.off + i;
+        const float4 me = sbody[p];
+        const double tx = me.x, ty = me.y;
+        const double eps2 = __dmul_rn(eps, eps);
+        const double root_half = simout[sim].half;
+        double ax = 0.0, ay = 0.0, s = 0.0;
+        auto add = [&](double x, double y, double mass) {
+            const double dx = __dsub_rn(x, tx);
+            const double dy = __dsub_rn(y, ty);
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), eps2);
+            const double inv_r = __ddiv_rn(1.0, __dsqrt_rn(r2));
+            const double scale =
+                __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(g, mass), inv_r), inv_r), inv_r);
+            const double fx = __dmul_rn(dx, scale), fy = __dmul_rn(dy, scale);
+            ax = __dadd_rn(ax, fx);
+            ay = __dadd_rn(ay, fy);
+            if (abs_sum) s += hypot(fx, fy);
+        };
+        const uint32_t root = base[sd.off];
+        const uint32_t stop = cell_u[root].y;  // the root's skip: past the last cell
+        uint32_t k = root;
+        while (k < stop) {
+            const uint4 u = cell_u[k];  // (end, skip, start, depth)
+            ++nv;
+            if (u.y == k + 1u) {  // a leaf: its bodies directly, self excluded
+                for (uint32_t q = u.z; q < u.x; ++q) {
+                    if (q == p) continue;
+                    const float4 o = sbody[q];
+                    add((double)o.x, (double)o.y, (double)o.z);
+                    ++nd;
+                }
+                k = u.y;
+                continue;
+            }
+            const double4 c = cell_d[k];
+            const double dist = hypot(__dsub_rn(c.x, tx), __dsub_rn(c.y, ty));
+            const double width = __dmul_rn(__dmul_rn(root_half, pow2_neg(u.w)), 2.0);
+            const bool contains = p >= u.z && p < u.x;
+            if (!contains && dist > 0.0 && __ddiv_rn(width, dist) < theta) {
+                add(c.x, c.y, c.z);
+                ++na;
+                k = u.y;
+            } else {
+                k = k + 1u;  // open: the first child follows its parent
+            }
+        }
+        const uint32_t idx = __float_as_uint(me.w);
+        out[idx] = make_double2(ax, ay);
+        if (abs_sum) abs_sum[idx] = s;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nv += __shfl_xor_sync(kFull, nv, o);
+        na += __shfl_xor_sync(kFull, na, o);
+        nd += __shfl_xor_sync(kFull, nd, o);
+    }
+    if (stats && lane_id() == 0 && nv) {
+        atomicAdd(&stats[0], nv);
+        atomicAdd(&stats[1], na);
+        atomicAdd(&stats[2], nd);
+    }
+}
+
+cudaError_t launch_traverse_f64(const BatchBuffers& b, uint32_t sim, uint32_t n, double theta,
+                                double eps, double g, double* out, double* abs_sum,
+                                unsigned long long* stats, cudaStream_t s) {
+    const uint32_t blocks = (n + kF64Threads - 1) / kF64Threads;
+    if (blocks == 0) return cudaSuccess;
+    k_traverse_f64<<<blocks, kF64Threads, 0, s>>>(b.sims, b.simout, sim, b.sbody, b.cell_u,
+                                                  b.cell_d, b.base, theta, eps, g,
+                                                  reinterpret_cast<double2*>(out), abs_sum, stats);
+    return cudaGetLastError();
+}
+
 // ======================================================= conservation =====
 
 constexpr int kConsThreads = 256;
@@ -1740,19 +1941,32 @@ __global__ void k_conservation_final(const double* partials, uint32_t nblocks, d
 
 // ============================================================ launchers ===
 
+static int sm_count();
+
+// One resident wave of integrate blocks (each warp then streams a contiguous
+// run of chunks), fewer when there are fewer chunks than warps.
+template <int MODE>
 static uint32_t integrate_blocks(uint32_t nchunks) {
-    uint32_t blocks = (nchunks + 7) / 8;
-    const uint32_t cap = 148u * 8u;
+    static int per_sm[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& r = per_sm[dev & 63];
+    if (!r) {
+        int v = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_integrate<MODE>, 256, 0);
+        r = v > 0 ? v : 1;
+    }
+    const uint32_t cap = (uint32_t)(sm_count() * r);
+    const uint32_t blocks = (nchunks + 7) / 8;
     return blocks < cap ? (blocks ? blocks : 1u) : cap;
 }
 
 cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s) {
-    const uint32_t blocks = integrate_blocks(b.nchunks);
     switch (mode) {
-        case 0: return launch_step(k_integrate<0>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
-        case 1: return launch_step(k_integrate<1>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
-        case 2: return launch_step(k_integrate<2>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
-        default: return launch_step(k_integrate<3>, blocks, 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        case 0: return launch_step(k_integrate<0>, integrate_blocks<0>(b.nchunks), 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        case 1: return launch_step(k_integrate<1>, integrate_blocks<1>(b.nchunks), 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        case 2: return launch_step(k_integrate<2>, integrate_blocks<2>(b.nchunks), 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
+        default: return launch_step(k_integrate<3>, integrate_blocks<3>(b.nchunks), 256, 0, s, b.sims, b.chunk_sim, b.nchunks, b.minmax);
     }
     return cudaGetLastError();
 }
@@ -1844,11 +2058,15 @@ cudaError_t launch_refresh_mac(const BatchBuffers& b, uint32_t sim, cudaStream_t
 template <int WARPS>
 static cudaError_t traverse_launch(const BatchBuffers& b, bool compensated, bool potential,
                                    bool stats, cudaStream_t s) {
-    const uint32_t blocks = (b.nchunks + WARPS - 1) / WARPS;
+    // The compensated form keeps a residual per list entry; with it 8 warps'
+    // static shared memory would pass 48 KB, so it runs at most 4 warps per
+    // block (each warp does the same work at any block size).
+    constexpr int CW = WARPS > 4 ? 4 : WARPS;
 #define GBH_TRAVERSE(C, P, S)                                                                   \
-    return launch_step(k_traverse<C, P, S, WARPS>, blocks, WARPS * 32, 0, s, b.sims, b.simout,  \
-                       b.chunk_sim, b.nchunks, b.sbody, b.groups, b.cell_d, b.cell_capacity,    \
-                       b.force_stats, b.err)
+    return launch_step(k_traverse<C, P, S, (C ? CW : WARPS)>,                                   \
+                       (b.nchunks + (C ? CW : WARPS) - 1) / (C ? CW : WARPS),                   \
+                       (C ? CW : WARPS) * 32, 0, s, b.sims, b.simout, b.chunk_sim, b.nchunks,  \
+                       b.sbody, b.groups, b.cell_d, b.cell_capacity, b.force_stats, b.err)
     if (stats) {
         if (compensated) {
             if (potential) GBH_TRAVERSE(true, true, true);

@@ -85,7 +85,10 @@ static std::mutex g_setup_mutex;
 static double* g_scratch_address[kMaxDevices] = {};
 
 // Device address of g_conservation_scratch on the current device, looked up
-// once per device with that device current.
+// once per device with that device current.  The address belongs to the
+// device's context: a cudaDeviceReset in this process ends that context and
+// the cached address with it, so the entry point must not be called on a
+// device after a reset (the header says so).
 static int scratch_address(double** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -131,6 +134,25 @@ extern "C" int galaxy_bh_conservation_noalloc(const GpuEvolveState* state, const
     if (rc) return rc;
     const uint32_t blocks = (n + kSliceBodies - 1) / kSliceBodies;
     cudaStream_t s = (cudaStream_t)stream;
+    if (s) {
+        // the scratch address is the current device's: the stream must run there
+        int cur = -1, sdev = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e == cudaSuccess) e = cudaStreamGetDevice(s, &sdev);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            char msg[256];
+            snprintf(msg, sizeof msg, "stream device query failed: %s", cudaGetErrorName(e));
+            return gbh::set_error_message(BH_INVALID_ARG, msg);
+        }
+        if (sdev != cur) {
+            char msg[256];
+            snprintf(msg, sizeof msg,
+                     "stream belongs to device %d but device %d is current; make the "
+                     "stream's device current before the call", sdev, cur);
+            return gbh::set_error_message(BH_INVALID_ARG, msg);
+        }
+    }
     k_conservation_slices<<<blocks, kThreads, 0, s>>>(state, potential, n, scratch);
     k_conservation_rows<<<1, 32, 0, s>>>(scratch, blocks, sums);
     cudaError_t e = cudaGetLastError();

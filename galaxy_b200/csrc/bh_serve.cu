@@ -51,6 +51,7 @@ struct bh_server {
     std::condition_variable cv_in, cv_out;
     std::deque<std::unique_ptr<ServeRequest>> submitted, done;
     bool stopping = false;
+    int pollers = 0;  // polls inside galaxy_bh_serve_poll (stop waits for them)
     uint64_t next_id = 1;
     uint64_t rounds = 0, particle_steps = 0, completed = 0;
     double busy_s = 0.0;
@@ -262,16 +263,28 @@ extern "C" int galaxy_bh_serve_poll(bh_server* s, uint32_t timeout_ms, bh_serve_
     std::unique_ptr<ServeRequest> taken;
     {
         std::unique_lock<std::mutex> lk(s->mu);
-        if (!s->cv_out.wait_for(lk, std::chrono::milliseconds(timeout_ms),
-                                [&] { return !s->done.empty(); }))
-            return set_error_message(BH_TIMEOUT, "no finished request within the timeout");
+        if (s->stopping) return set_error_message(BH_INVALID_ARG, "server stopped");
+        ++s->pollers;
+        // leaves the wait on a result, on the timeout, or when stop begins
+        auto leave = [&](int status, const char* msg) {
+            --s->pollers;
+            s->cv_out.notify_all();
+            return set_error_message(status, msg);
+        };
+        const bool ready = s->cv_out.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] {
+            return !s->done.empty() || s->stopping;
+        });
+        if (s->stopping) return leave(BH_INVALID_ARG, "server stopped");
+        if (!ready) return leave(BH_TIMEOUT, "no finished request within the timeout");
         const ServeRequest& r = *s->done.front();
         res->request_id = r.id;
         res->n = r.n;
         if (r.status == BH_OK && (!out || capacity < r.n))  // kept for a retry with room
-            return set_error_message(BH_INVALID_ARG, "result buffer smaller than the request");
+            return leave(BH_INVALID_ARG, "result buffer smaller than the request");
         taken = std::move(s->done.front());
         s->done.pop_front();
+        --s->pollers;
+        s->cv_out.notify_all();
     }
     // the copy and the release of the records run without the server's lock
     const ServeRequest& r = *taken;
@@ -301,8 +314,14 @@ extern "C" int galaxy_bh_serve_stop(bh_server* s) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stopping = true;
         s->cv_in.notify_all();
+        s->cv_out.notify_all();  // waiting polls return "server stopped"
     }
     if (s->loop.joinable()) s->loop.join();
+    {
+        // no poll may still be inside the server when it is freed
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_out.wait(lk, [&] { return s->pollers == 0; });
+    }
     galaxy_bh_device_close(s->dev);
     delete s;
     return BH_OK;

@@ -431,6 +431,17 @@ class ParallelGpuTreeEvidence:
     leaf_count: int
     max_depth: int
 
+    def packed(self, config: Config) -> PackedFlat:
+        """The BH #2B1 packed flat tree (nbody_gpu.rs:175-250) of this
+        evidence: the same records pack_flat_tree writes for the
+        reference's CPU tree of the same bodies (root cell 0)."""
+        settings = np.zeros((), _lib.BH_SETTINGS_DTYPE)
+        settings["info"] = [len(self.bodies), self.active_cell_count, 0, 0]
+        settings["physics"] = [_checked_f32(config.theta, "theta"),
+                               _checked_f32(config.softening_kpc, "softening_kpc"),
+                               _checked_f32(config.g, "G"), 0.0]
+        return PackedFlat(settings, self.bodies, self.entries, self.cells)
+
 
 class ParallelTreeRuntime:
     """nbody_parallel.rs:93-993: GPU tree construction, force and evidence."""
@@ -480,6 +491,24 @@ class ParallelTreeRuntime:
         return {"visited_nodes": s.visited_nodes, "approximated_cells": s.approximated_cells,
                 "direct_terms": s.direct_terms, "exact_mac_fallbacks": s.exact_mac_fallbacks,
                 "warp_iterations": s.warp_iterations}
+
+    def force_f64(self, gpu: NbodyGpu, evolving: EvolvingState, tree: ParallelGpuTree,
+                  config: Config, abs_sum: bool = False):
+        """flat_accelerations_from_tree (nbody/src/flat.rs:270-371) in f64 on
+        the device over the tree of the last rebuild: (n, 2) accelerations in
+        resident order, the per-body sum of term magnitudes (or None) and the
+        reference's force counters."""
+        n = evolving.count
+        acc = np.zeros((n, 2))
+        s = np.zeros(n) if abs_sum else None
+        st = BhForceStats()
+        c = config.to_c()
+        check(_lib.load().galaxy_bh_force_f64(gpu.handle, evolving.handle, tree.handle,
+                                              C.byref(c), ptr(acc),
+                                              ptr(s) if s is not None else None, C.byref(st)))
+        return acc, s, {"visited_nodes": st.visited_nodes,
+                        "approximated_cells": st.approximated_cells,
+                        "direct_terms": st.direct_terms}
 
     def step(self, gpu: NbodyGpu, evolving: EvolvingState, tree: ParallelGpuTree,
              config: Config, dt_myr: float, steps: int) -> None:

@@ -195,6 +195,18 @@ int galaxy_bh_force(bh_device* dev, bh_state* st, bh_tree* tree, const bh_config
                     bh_stage_timing* timing);
 /* Counters of the last galaxy_bh_force on this tree. */
 int galaxy_bh_force_stats(bh_device* dev, bh_tree* tree, bh_force_stats* out);
+/* The reference's CPU flat traversal, flat_accelerations_from_tree
+ * (nbody/src/flat.rs:270-371), in f64 on the device over the tree of the
+ * last rebuild: the same cells in the same depth-first order, the same f64
+ * aggregates, MAC and per-term arithmetic (lib.rs:247-255), so each body's
+ * sum repeats the reference's additions.  accel receives ax, ay per body
+ * (2n doubles, resident order, host memory); abs_sum (n doubles, or NULL)
+ * the sum of each body's term magnitudes; stats (or NULL) the reference's
+ * visited / approximated / direct counters.  cfg supplies theta, softening
+ * and G in f64.  It states the per-body error of the f32 forces at full
+ * size without a CPU pass; it does not touch the state's accelerations. */
+int galaxy_bh_force_f64(bh_device* dev, bh_state* st, bh_tree* tree, const bh_config* cfg,
+                        double* accel, double* abs_sum, bh_force_stats* stats);
 /* ParallelTreeRuntime::read_evidence (nbody_parallel.rs:929-988): meta,
  * sorted entries (n), bodies with Morton positions (n), and the cells in
  * the reference CPU preorder (flat.rs:127-177) in the frozen 64-byte
@@ -258,13 +270,19 @@ int galaxy_bh_conservation(bh_device* dev, bh_state* st, double out[10]);
  * (n GpuEvolveState records) and potential (n floats, or NULL) are device
  * inputs; sums is a device output of 9 doubles — mass, sum m*x, sum m*y, px,
  * py, lz, kinetic, potential, sum m*|v| (divide 1 and 2 by 0 for the centre
- * of mass).  Work is enqueued on `stream` (a cudaStream_t; NULL = default
- * stream) and the function returns without waiting.  Scratch is a 73,728-byte
- * static device array, so n is limited to 4,194,304 (BH_INVALID_ARG beyond).
- * The first call on each device looks up that array's device address with
- * the device current; make that first call before any stream capture.  All
- * calls share the one array: calls that overlap on the GPU (different streams
- * or threads at once) race and corrupt each other's sums. */
+ * of mass).  Work is enqueued on `stream` (a cudaStream_t of the current
+ * device, BH_INVALID_ARG otherwise) and the function returns without
+ * waiting.  NULL means the legacy default stream, which is NOT ordered after
+ * this library's own streams (they are non-blocking): when state comes from
+ * an engine call, order this call after it yourself (an event, or a
+ * synchronize).  Scratch is a 73,728-byte static device array, so n is
+ * limited to 4,194,304 (BH_INVALID_ARG beyond).  The first call on each
+ * device looks up that array's device address with the device current; make
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process: after a cudaDeviceReset of a device, do not call this
+ * function on that device again.  All calls share the one array: calls that
+ * overlap on the GPU (different streams or threads at once) race and
+ * corrupt each other's sums. */
 int galaxy_bh_conservation_noalloc(const GpuEvolveState* state, const float* potential,
                                    uint32_t n, double* sums, void* stream);
 
@@ -303,7 +321,10 @@ int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
  * sets result->request_id and result->n and keeps the result queued).
  * submit, poll and stats may be called from
  * any host thread; stop ends the loop after the current round, drops
- * unfinished requests and frees everything. */
+ * unfinished requests (submitted, waiting and active ones get no result),
+ * makes polls that are waiting return BH_INVALID_ARG ("server stopped"),
+ * waits for them to leave and frees everything; the handle must not be used
+ * after stop returns. */
 typedef struct bh_server bh_server;
 typedef struct {
     uint64_t budget_bytes;

@@ -77,8 +77,9 @@ def build_oracle() -> None:
     """Compile liboracle_bh.so (and the reference CUDA shim when the
     reference tree is present) with the committed Makefile."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=False)
+    ref = os.environ.get("GALAXY_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=False)
 
 
 _lib = None
@@ -471,6 +472,8 @@ def ref_cuda():
                                       C.POINTER(C.c_float), C.c_int]
         L.ref_bh_kick_drift.argtypes = [P, P, C.c_uint32, C.c_float]
         L.ref_bh_final_kick.argtypes = [P, P, C.c_uint32, C.c_float]
+        L.ref_bh_integrate_timed.argtypes = [C.c_int, P, P, C.c_uint32, C.c_float,
+                                             C.POINTER(C.c_float), C.c_int]
         _ref = L
     return _ref
 
@@ -485,6 +488,20 @@ def ref_cuda_traverse(p: Packed, repeats=1):
     if rc:
         raise OracleError(f"reference CUDA traversal failed: cudaError {rc}")
     return out, float(ms.value)
+
+
+def ref_cuda_integrate_timed(states, accel, dt, final_kick=False, repeats=5):
+    """The reference's bh_kick_drift / bh_final_kick over (states, accel):
+    (states after one launch, mean device ms of `repeats` further launches)."""
+    L = ref_cuda()
+    s = np.ascontiguousarray(states, dtype=np.float32).copy()
+    a = np.ascontiguousarray(accel, dtype=np.float32)
+    ms = C.c_float(0.0)
+    rc = L.ref_bh_integrate_timed(int(final_kick), _ptr(s), _ptr(a), len(s), np.float32(dt),
+                                  C.byref(ms), repeats)
+    if rc:
+        raise OracleError(f"reference CUDA integrate failed: cudaError {rc}")
+    return s, float(ms.value)
 
 
 def ref_cuda_integrate(states, accel, dt, final_kick=False):

@@ -58,7 +58,8 @@ done:
     return (int)err;
 }
 
-static int run_integrate(int final_kick, void* states, const void* accel, uint32_t n, float dt) {
+static int run_integrate(int final_kick, void* states, const void* accel, uint32_t n, float dt,
+                         float* kernel_ms, int repeats) {
     EvolveSettings s = {};
     s.info[0] = n;
     s.motion[0] = dt;
@@ -79,15 +80,40 @@ static int run_integrate(int final_kick, void* states, const void* accel, uint32
         bh_kick_drift<<<(n + 127) / 128, 128>>>(d_s, d_st, d_a);
     if ((err = cudaGetLastError())) goto done;
     err = cudaMemcpy(states, d_st, sizeof(EvolveState) * (size_t)n, cudaMemcpyDeviceToHost);
+    if (!err && kernel_ms) {
+        // further launches on the device copy, timed (the state keeps moving)
+        Timer t;
+        if (repeats < 1) repeats = 1;
+        cudaEventRecord(t.a);
+        for (int r = 0; r < repeats; ++r) {
+            if (final_kick)
+                bh_final_kick<<<(n + 127) / 128, 128>>>(d_s, d_st, d_a);
+            else
+                bh_kick_drift<<<(n + 127) / 128, 128>>>(d_s, d_st, d_a);
+        }
+        cudaEventRecord(t.b);
+        if ((err = cudaEventSynchronize(t.b))) goto done;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        *kernel_ms = ms / (float)repeats;
+        err = cudaGetLastError();
+    }
 done:
     cudaFree(d_s); cudaFree(d_st); cudaFree(d_a);
     return (int)err;
 }
 
 extern "C" int ref_bh_kick_drift(void* states, const void* accel, uint32_t n, float dt) {
-    return run_integrate(0, states, accel, n, dt);
+    return run_integrate(0, states, accel, n, dt, nullptr, 0);
 }
 
 extern "C" int ref_bh_final_kick(void* states, const void* accel, uint32_t n, float dt) {
-    return run_integrate(1, states, accel, n, dt);
+    return run_integrate(1, states, accel, n, dt, nullptr, 0);
+}
+
+// One launch whose result goes to `states`, then `repeats` timed launches on
+// the device copy; *kernel_ms = mean device time of those.
+extern "C" int ref_bh_integrate_timed(int final_kick, void* states, const void* accel, uint32_t n,
+                                      float dt, float* kernel_ms, int repeats) {
+    return run_integrate(final_kick, states, accel, n, dt, kernel_ms, repeats);
 }

@@ -17,7 +17,8 @@ import re
 import subprocess
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = (sys.argv[1] if len(sys.argv) > 1 else
+       os.environ.get("GALAXY_REFERENCE_DIR", "/root/reference"))
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_vectors.json")
 
 

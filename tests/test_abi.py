@@ -114,9 +114,28 @@ def test_host_state_validation():
         Config(bucket=0).validate()
 
 
-def test_integration_rust_block_covers_the_header():
-    """INTEGRATION.md's Rust extern blocks declare every function of the
-    header, so a maintainer wiring the runtime binds the whole surface."""
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    rust = set(re.findall(r"fn (galaxy_bh_[a-z0-9_]+)\(", text))
-    assert set(declared_symbols()) <= rust, sorted(set(declared_symbols()) - rust)
+def _arity(params: str) -> int:
+    params = params.strip()
+    if params in ("", "void"):
+        return 0
+    return len([x for x in params.split(",") if x.strip()])
+
+
+def header_declarations() -> dict:
+    """name -> parameter count of every function declared in the header."""
+    text = open(os.path.join(ROOT, "include", "galaxy_bh.h")).read()
+    return {m[0]: _arity(m[1]) for m in re.findall(
+        r"\b(?:int|uint32_t|size_t)\s+(galaxy_bh_\w+)\s*\(([^)]*)\)\s*;", text)}
+
+
+def test_rust_crate_binds_the_whole_header():
+    """The Rust crate (galaxy_b200/rust) declares every function of the
+    header with the same parameter count, so a maintainer wiring the
+    reference's runtime binds the whole surface."""
+    decl = header_declarations()
+    assert set(decl) == set(declared_symbols())
+    src = open(os.path.join(ROOT, "galaxy_b200", "rust", "src", "lib.rs")).read()
+    rust = {m[0]: _arity(m[1]) for m in re.findall(r"pub fn (galaxy_bh_\w+)\(([^)]*)\)", src)}
+    assert set(rust) == set(decl), sorted(set(rust) ^ set(decl))
+    for name, n in decl.items():
+        assert rust[name] == n, (name, rust[name], n)

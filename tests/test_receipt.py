@@ -95,3 +95,57 @@ def test_validator_rejects(path, value):
     d[path[-1]] = value
     with pytest.raises(receipt.ReceiptError):
         receipt.validate_receipt(r, **WORK)
+
+
+def _reference_sweep_module():
+    """The reference's scripts/bench-bh2d-hardware.py, imported from the
+    reference tree (present where fixtures are made, absent on GPU hosts)."""
+    import importlib.util
+    import os
+    ref = os.environ.get("GALAXY_REFERENCE_DIR", "/root/reference")
+    path = os.path.join(ref, "scripts", "bench-bh2d-hardware.py")
+    if not os.path.exists(path):
+        pytest.skip("reference tree absent")
+    spec = importlib.util.spec_from_file_location("reference_bh2d_sweep", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_reference_sweep_validator_accepts_engine_receipts(monkeypatch):
+    """Receipts this engine produced on a GPU (tests/golden/engine_receipts.json,
+    made by tests/golden/make_engine_receipts.py) pass the reference's OWN
+    validate_receipt (scripts/bench-bh2d-hardware.py:1013), with exactly two
+    documented substitutions: the backend set admits "CUDA" (:993 admits
+    Vulkan / Metal / Dx12), and the tree-buffer formula (:837-853, the
+    reference's 17 N sparse 64-byte cells) is this engine's
+    galaxy_bh_tree_footprint.  Every other check is the reference's code."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "engine_receipts.json")
+    if not os.path.exists(path):
+        pytest.skip("engine receipts not generated yet")
+    mod = _reference_sweep_module()
+    backend_msg = "receipt.gpu.backend is not enabled by the producer"
+    real_require = mod.require
+    seen = {"backend": 0}
+
+    def require(condition, message):
+        if message == backend_msg and not condition:
+            seen["backend"] += 1
+            return  # "CUDA": the one backend the reference set does not list
+        real_require(condition, message)
+
+    monkeypatch.setattr(mod, "require", require)
+    monkeypatch.setattr(mod, "expected_parallel_tree_buffer_bytes",
+                        lambda n: receipt.tree_footprint_bytes(n, Config()))
+    cases = json.load(open(path))
+    assert len(cases) >= 2
+    for case in cases:
+        assert case["receipt"]["gpu"]["backend"] == "CUDA"
+        mod.validate_receipt(case["receipt"], **case["workload"])
+    assert seen["backend"] == len(cases)
+    # the unpatched validator rejects exactly on the backend
+    monkeypatch.setattr(mod, "require", real_require)
+    with pytest.raises(mod.SweepError, match="backend"):
+        mod.validate_receipt(cases[0]["receipt"], **cases[0]["workload"])

@@ -85,3 +85,34 @@ def test_noalloc_potential_and_limits():
     assert rc == _lib.BH_INVALID_ARG
     assert "4194304" in _lib.last_error()
     assert lib.galaxy_bh_conservation_noalloc(None, None, 10, None, None) == _lib.BH_INVALID_ARG
+
+
+def test_noalloc_at_the_limit_allocates_nothing():
+    """n = 4,194,304 fills every scratch row; the sums equal the existing
+    entry point's, and a repeated call on buffers the caller already holds
+    leaves the device's free memory unchanged."""
+    import torch
+
+    from galaxy_b200 import _lib, scenarios
+    from galaxy_b200.nbody_gpu import NbodyGpu, bodies_to_state
+    lib = _lib.load()
+    n = 4_194_304
+    recs = bodies_to_state(scenarios.binary_encounter(n, 13))
+    d_state = _device_records(torch, recs)
+    d_sums = torch.full((9,), float("nan"), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def call():
+        _lib.check(lib.galaxy_bh_conservation_noalloc(
+            C.c_void_p(d_state.data_ptr()), None, n, C.c_void_p(d_sums.data_ptr()),
+            C.c_void_p(stream.cuda_stream)))
+        stream.synchronize()
+        return d_sums.cpu().numpy()
+
+    first = call()
+    free_before, _ = torch.cuda.mem_get_info()
+    second = call()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    assert np.array_equal(first, second)
+    _compare(second, _existing(NbodyGpu("0"), recs))
