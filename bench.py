@@ -214,8 +214,10 @@ def reference_kernels(s) -> dict | None:
     """The reference's own CUDA kernels (runtime/cuda/barnes_hut_flat.cu,
     compiled unmodified from its source into oracle/_ref): bh_traverse over
     the packed tree of the workload's initial state (its CPU tree,
-    pack_flat_tree), bh_kick_drift and bh_final_kick over the same bodies;
-    mean device ms of repeated launches.  None when they were not built."""
+    pack_flat_tree), bh_kick_drift and bh_final_kick over the same bodies, in
+    128-thread groups as nbody_gpu.rs dispatches them.  Median device ms of
+    single launches, each bracketed by its own events, with L2 warm and with
+    L2 evicted before each launch (cold).  None when they were not built."""
     from galaxy_b200.nbody_gpu import state_to_bodies
     from oracle import oracle
     if oracle.ref_cuda() is None:
@@ -224,16 +226,18 @@ def reference_kernels(s) -> dict | None:
     cfg = oracle.Config(theta=THETA, softening=EPS, g=G, bucket=BUCKET, max_depth=48)
     tree = oracle.build_flat_tree(b, cfg)
     packed = oracle.pack_flat_tree(b, tree, cfg)
-    acc, t_ms = oracle.ref_cuda_traverse(packed, repeats=5)
-    recs = s.view(np.float32).reshape(-1, 8)
-    _, kd_ms = oracle.ref_cuda_integrate_timed(recs, acc, DT, final_kick=False, repeats=5)
-    _, fk_ms = oracle.ref_cuda_integrate_timed(recs, acc, DT, final_kick=True, repeats=5)
-    return {"tree": f"initial state of the workload (cold disc 2^20, seed 7), "
-                    f"{len(packed.cells)} cells",
-            "source": "runtime/cuda/barnes_hut_flat.cu (bh_traverse, bh_kick_drift, "
-                      "bh_final_kick), 128-thread groups as nbody_gpu.rs dispatches them",
-            "traverse_ms": float(f"{t_ms:.4g}"), "kick_drift_ms": float(f"{kd_ms:.4g}"),
-            "final_kick_ms": float(f"{fk_ms:.4g}")}
+    acc, _ = oracle.ref_cuda_traverse(packed, repeats=1)
+    t = oracle.ref_cuda_single_times(packed, s.view(np.float32).reshape(-1, 8), acc, DT)
+    out = {"tree": f"initial state of the workload (cold disc 2^20, seed 7), "
+                   f"{len(packed.cells)} cells",
+           "source": "runtime/cuda/barnes_hut_flat.cu (bh_traverse, bh_kick_drift, "
+                     "bh_final_kick), 128-thread groups as nbody_gpu.rs dispatches them",
+           "how": "median of single launches, device time (CUDA events); cold = L2 evicted "
+                  "before each launch"}
+    for k, (w, c) in t.items():
+        out[k + "_ms"] = float(f"{w:.4g}")
+        out[k + "_cold_ms"] = float(f"{c:.4g}")
+    return out
 
 
 def run_reference(args, world, rank, pg):
@@ -414,28 +418,54 @@ def per_body_force_error(gpu, rt, ev, tree, cfg) -> dict:
     return out
 
 
-def same_tree_kernels(gpu, rt, s0, cfg, reps: int = 3) -> dict:
+def same_tree_kernels(gpu, rt, s0, cfg, reps: int = 7) -> dict:
     """This engine's kernels on the tree of the workload's initial state,
     the tree the reference arm hands the reference's own CUDA kernels
     (runtime/cuda/barnes_hut_flat.cu): the BH #2B1 packed traversal of the
     same packed records (galaxy_bh_traverse_packed), the engine's own
     traversal of that tree (galaxy_bh_force), and the kick/drift (with the
-    fused bounds reduction) and final kick.  Best of `reps` device times."""
+    fused bounds reduction) and final kick.  Median device ms of `reps`
+    single calls, each kernel bracketed by its own events, as the reference
+    arm times the reference's kernels: "warm" right after the previous call,
+    "cold" after a 256 MiB write that evicts L2 (the packed traversal
+    uploads its tree first, so it has only the one figure)."""
+    import torch
     ev, _ = gpu.create_evolving_state_records(s0)
     tree = rt.create_tree(gpu, ev, cfg)
     rt.rebuild(gpu, ev, tree, cfg)
     packed = rt.read_evidence(gpu, tree).packed(cfg)
     plain = dataclasses.replace(cfg, force_stats=False)
-    t_packed = min(gpu.traverse(packed).dispatch_seconds for _ in range(reps))
-    t_force = min(rt.force(gpu, ev, tree, plain).dispatch_seconds for _ in range(reps))
-    t_kd = min(gpu.kick_drift(ev, DT).dispatch_seconds for _ in range(reps))
-    t_fk = min(gpu.final_kick(ev, DT).dispatch_seconds for _ in range(reps))
+    stream = torch.cuda.ExternalStream(gpu.stream_ptr())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(call, cold):
+        out = []
+        for r in range(reps):
+            if cold:
+                with torch.cuda.stream(stream):
+                    flush.fill_(r & 0xFF)
+            out.append(call() * 1e3)
+        return r4(float(np.median(out)))
+
+    res = {"tree": "initial state of the workload (cold disc 2^20, seed 7), "
+                   f"{len(packed.cells)} cells",
+           "how": "median of single calls, device time of the kernel (CUDA events); cold = "
+                  "L2 evicted before each call"}
+    res["traverse_packed_ms"] = timed(lambda: gpu.traverse(packed).dispatch_seconds, False)
+    for cold in (False, True):
+        sfx = "_cold_ms" if cold else "_ms"
+        res["traverse" + sfx] = timed(lambda: rt.force(gpu, ev, tree, plain).dispatch_seconds,
+                                      cold)
+        res["kick_drift" + sfx] = timed(lambda: gpu.kick_drift(ev, DT).dispatch_seconds, cold)
+        res["final_kick" + sfx] = timed(lambda: gpu.final_kick(ev, DT).dispatch_seconds, cold)
+        # the pass the fused step runs between steps: final kick + kick/drift
+        # + bounds, against the reference's two launches per step
+        res["final_kick_drift" + sfx] = timed(
+            lambda: gpu.final_kick_drift(ev, DT).dispatch_seconds, cold)
+    del flush
     tree.close()
     ev.close()
-    return {"tree": "initial state of the workload (cold disc 2^20, seed 7), "
-                    f"{len(packed.cells)} cells",
-            "traverse_packed_ms": r4(t_packed * 1e3), "traverse_ms": r4(t_force * 1e3),
-            "kick_drift_ms": r4(t_kd * 1e3), "final_kick_ms": r4(t_fk * 1e3)}
+    return res
 
 
 def run_engine(args, world, rank, local, pg):

@@ -123,6 +123,7 @@ SIGNATURES = {
     "galaxy_bh_state_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "galaxy_bh_kick_drift": (C.c_int, [_P, _P, C.c_double, C.POINTER(BhStageTiming)]),
     "galaxy_bh_final_kick": (C.c_int, [_P, _P, C.c_double, C.POINTER(BhStageTiming)]),
+    "galaxy_bh_final_kick_drift": (C.c_int, [_P, _P, C.c_double, C.POINTER(BhStageTiming)]),
     "galaxy_bh_read_state": (C.c_int, [_P, _P, _P, _U32, C.POINTER(BhStageTiming)]),
     "galaxy_bh_read_accel": (C.c_int, [_P, _P, _P, _U32, C.POINTER(BhStageTiming)]),
     "galaxy_bh_write_state": (C.c_int, [_P, _P, _P, _U32]),

@@ -393,6 +393,11 @@ extern "C" int galaxy_bh_final_kick(bh_device* dev, bh_state* st, double dt,
     return integrate_state(dev, st, dt, 2, timing);
 }
 
+extern "C" int galaxy_bh_final_kick_drift(bh_device* dev, bh_state* st, double dt,
+                                          bh_stage_timing* timing) {
+    return integrate_state(dev, st, dt, 3, timing);
+}
+
 // Enqueues the record check of n records at `records` (kind 0: evolving
 // states, 1: accelerations) and the copy of its result word to *first_bad.
 static int enqueue_check(bh_state* st, const void* records, int kind, uint32_t n) {

@@ -200,7 +200,10 @@ constexpr long long kSpinCycles = 2000000000ll;
 // final kick of one step and the kick-drift of the next with the same two
 // roundings as two separate launches.  Modes 0, 1, 3 also reduce the
 // per-simulation f32 bounds of the (new) positions.
-constexpr int kIntegrateUnroll = 4;  // chunks whose loads a warp keeps in flight
+#ifndef GBH_INTEGRATE_UNROLL
+#define GBH_INTEGRATE_UNROLL 4
+#endif
+constexpr int kIntegrateUnroll = GBH_INTEGRATE_UNROLL;  // chunks whose loads a warp keeps in flight
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ sims,
@@ -211,11 +214,10 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
     __shared__ uint32_t s_sim[8];
     __shared__ float s_val[8][4];
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    // each warp streams a contiguous run of chunks
+    // grid-stride over chunks, kIntegrateUnroll strides per round: at any
+    // moment the warps of the grid stream one contiguous region
     const uint32_t nwarps = gridDim.x * 8;
-    const uint32_t per = (nchunks + nwarps - 1) / nwarps;
-    const uint32_t c_begin = min((blockIdx.x * 8 + warp) * per, nchunks);
-    const uint32_t c_end = min(c_begin + per, nchunks);
+    const uint32_t gw = blockIdx.x * 8 + warp;
     uint32_t cur = kNone;
     // fields of simulation `cur`, reloaded only when the simulation changes
     GpuEvolveState* st = nullptr;
@@ -293,19 +295,21 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
         bound(pm);
     };
 
-    constexpr uint32_t kPast = kNone - 1u;  // a slot past the warp's last chunk
-    for (uint32_t chunk = c_begin; chunk < c_end; chunk += kIntegrateUnroll) {
-        uint32_t sv[kIntegrateUnroll];
+    constexpr uint32_t kPast = kNone - 1u;  // a slot past the last chunk
+    for (uint32_t round = gw; round < nchunks; round += kIntegrateUnroll * nwarps) {
+        uint32_t sv[kIntegrateUnroll], cv[kIntegrateUnroll];
 #pragma unroll
-        for (int j = 0; j < kIntegrateUnroll; ++j)
-            sv[j] = chunk + j < c_end ? chunk_sim[chunk + j] : kPast;
+        for (int j = 0; j < kIntegrateUnroll; ++j) {
+            cv[j] = round + (uint32_t)j * nwarps;
+            sv[j] = cv[j] < nchunks ? chunk_sim[cv[j]] : kPast;
+        }
         bool same = sv[0] != kNone;
 #pragma unroll
         for (int j = 1; j < kIntegrateUnroll; ++j) same = same && (sv[j] == sv[0] || sv[j] == kPast);
         if (!same) {
 #pragma unroll 1
             for (int j = 0; j < kIntegrateUnroll; ++j)
-                if (sv[j] != kPast) one_chunk(chunk + j, sv[j]);
+                if (sv[j] != kPast) one_chunk(cv[j], sv[j]);
             continue;
         }
         // one simulation: every load of the run first, then the updates
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
         bool ok[kIntegrateUnroll];
 #pragma unroll
         for (int j = 0; j < kIntegrateUnroll; ++j) {
-            const uint32_t i = (chunk + j) * kChunk + lane - off;
+            const uint32_t i = cv[j] * kChunk + lane - off;
             ok[j] = sv[j] != kPast && i < n;
             if (ok[j]) {
                 const float4* rec = reinterpret_cast<const float4*>(st + i);
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
 #pragma unroll
         for (int j = 0; j < kIntegrateUnroll; ++j) {
             if (!ok[j]) continue;
-            const uint32_t i = (chunk + j) * kChunk + lane - off;
+            const uint32_t i = cv[j] * kChunk + lane - off;
             if (MODE != 0) {
                 update(pm[j], v[j], a[j]);
                 float4* rec = reinterpret_cast<float4*>(st + i);
@@ -1956,7 +1960,11 @@ static uint32_t integrate_blocks(uint32_t nchunks) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_integrate<MODE>, 256, 0);
         r = v > 0 ? v : 1;
     }
+#ifdef GBH_INTEGRATE_BLOCKS_PER_SM
+    const uint32_t cap = (uint32_t)(sm_count() * GBH_INTEGRATE_BLOCKS_PER_SM);
+#else
     const uint32_t cap = (uint32_t)(sm_count() * r);
+#endif
     const uint32_t blocks = (nchunks + 7) / 8;
     return blocks < cap ? (blocks ? blocks : 1u) : cap;
 }

@@ -336,6 +336,14 @@ class NbodyGpu:
                                                C.byref(t)))
         return StageTiming.of(t)
 
+    def final_kick_drift(self, evolving: EvolvingState, dt_myr: float) -> StageTiming:
+        """final_kick then kick_drift in one pass, bit-identical to the two
+        calls (what the fused step runs between steps)."""
+        t = BhStageTiming()
+        check(_lib.load().galaxy_bh_final_kick_drift(self._h.p, evolving.handle, float(dt_myr),
+                                                     C.byref(t)))
+        return StageTiming.of(t)
+
     def read_evolving_state_records(self, evolving: EvolvingState):
         out = np.zeros(evolving.count, _lib.EVOLVE_STATE_DTYPE)
         t = BhStageTiming()

@@ -216,6 +216,8 @@ pub mod ffi {
                                     timing: *mut BhStageTiming) -> c_int;
         pub fn galaxy_bh_final_kick(dev: *mut bh_device, st: *mut bh_state, dt: f64,
                                     timing: *mut BhStageTiming) -> c_int;
+        pub fn galaxy_bh_final_kick_drift(dev: *mut bh_device, st: *mut bh_state, dt: f64,
+                                          timing: *mut BhStageTiming) -> c_int;
         pub fn galaxy_bh_read_state(dev: *mut bh_device, st: *mut bh_state,
                                     out: *mut GpuEvolveState, n: u32,
                                     timing: *mut BhStageTiming) -> c_int;
@@ -393,6 +395,13 @@ impl Device {
     pub fn final_kick(&self, s: &EvolvingState<'_>, dt: f64) -> Result<BhStageTiming> {
         let mut t = BhStageTiming::default();
         check(unsafe { ffi::galaxy_bh_final_kick(self.raw, s.raw, dt, &mut t) })?;
+        Ok(t)
+    }
+
+    /// final_kick then kick_drift in one pass (bit-identical to the two calls).
+    pub fn final_kick_drift(&self, s: &EvolvingState<'_>, dt: f64) -> Result<BhStageTiming> {
+        let mut t = BhStageTiming::default();
+        check(unsafe { ffi::galaxy_bh_final_kick_drift(self.raw, s.raw, dt, &mut t) })?;
         Ok(t)
     }
 

@@ -164,6 +164,13 @@ int galaxy_bh_state_bytes(bh_state* st, uint64_t* bytes);
 /* NbodyGpu::kick_drift / final_kick (nbody_gpu.rs:1011-1017). */
 int galaxy_bh_kick_drift(bh_device* dev, bh_state* st, double dt, bh_stage_timing* timing);
 int galaxy_bh_final_kick(bh_device* dev, bh_state* st, double dt, bh_stage_timing* timing);
+/* final_kick(dt) then kick_drift(dt) (nbody_gpu.rs:1011-1017, in the order
+ * the reference loop calls them between two steps, galaxy-bh-gpu-tree-
+ * parallel.rs:345-350) in one pass over the records, with the same two f32
+ * roundings as the two calls: the results equal final_kick followed by
+ * kick_drift bit for bit.  galaxy_bh_step runs this pass between steps. */
+int galaxy_bh_final_kick_drift(bh_device* dev, bh_state* st, double dt,
+                               bh_stage_timing* timing);
 /* NbodyGpu::read_evolving_state (nbody_gpu.rs:1019-1069); fails with
  * BH_NONFINITE on non-finite values or mass <= 0 like the reference, naming
  * the first such record (checked on the device while the copy runs; `out`

@@ -474,6 +474,10 @@ def ref_cuda():
         L.ref_bh_final_kick.argtypes = [P, P, C.c_uint32, C.c_float]
         L.ref_bh_integrate_timed.argtypes = [C.c_int, P, P, C.c_uint32, C.c_float,
                                              C.POINTER(C.c_float), C.c_int]
+        L.ref_bh_integrate_single.argtypes = [C.c_int, P, P, C.c_uint32, C.c_float,
+                                              C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int]
+        L.ref_bh_traverse_single.argtypes = [P, P, C.c_uint32, P, P, C.c_uint32,
+                                             C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int]
         _ref = L
     return _ref
 
@@ -502,6 +506,30 @@ def ref_cuda_integrate_timed(states, accel, dt, final_kick=False, repeats=5):
     if rc:
         raise OracleError(f"reference CUDA integrate failed: cudaError {rc}")
     return s, float(ms.value)
+
+
+def ref_cuda_single_times(p: Packed, states, accel, dt, repeats=7) -> dict:
+    """Median single-launch device ms of the reference's bh_traverse (over
+    the packed tree p), bh_kick_drift and bh_final_kick (over states,
+    accel), each with L2 warm and with L2 flushed before every launch."""
+    L = ref_cuda()
+    out = {}
+    w, c = C.c_float(0.0), C.c_float(0.0)
+    rc = L.ref_bh_traverse_single(_ptr(p.settings), _ptr(p.bodies), len(p.bodies),
+                                  _ptr(p.entries), _ptr(p.cells), len(p.cells), C.byref(w),
+                                  C.byref(c), repeats)
+    if rc:
+        raise OracleError(f"reference CUDA traversal failed: cudaError {rc}")
+    out["traverse"] = (float(w.value), float(c.value))
+    s = np.ascontiguousarray(states, dtype=np.float32)
+    a = np.ascontiguousarray(accel, dtype=np.float32)
+    for name, fk in (("kick_drift", 0), ("final_kick", 1)):
+        rc = L.ref_bh_integrate_single(fk, _ptr(s), _ptr(a), len(s), np.float32(dt), C.byref(w),
+                                       C.byref(c), repeats)
+        if rc:
+            raise OracleError(f"reference CUDA integrate failed: cudaError {rc}")
+        out[name] = (float(w.value), float(c.value))
+    return out
 
 
 def ref_cuda_integrate(states, accel, dt, final_kick=False):

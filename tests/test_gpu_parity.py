@@ -204,6 +204,28 @@ def test_kick_drift_final_kick_bit_exact(gpu, oracle):
         np.testing.assert_allclose(r, want, rtol=5e-7, atol=2e-9)
 
 
+def test_final_kick_drift_equals_the_two_calls(gpu, rt):
+    """galaxy_bh_final_kick_drift (one pass) leaves the records bit-identical
+    to galaxy_bh_final_kick followed by galaxy_bh_kick_drift."""
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    bodies = scenarios.exponential_disc(7000, 4)
+    out = []
+    for fused in (False, True):
+        ev, _ = gpu.create_evolving_state(bodies)
+        tree = rt.create_tree(gpu, ev, cfg)
+        rt.rebuild(gpu, ev, tree, cfg)
+        rt.force(gpu, ev, tree, cfg)
+        if fused:
+            gpu.final_kick_drift(ev, 2e-3)
+        else:
+            gpu.final_kick(ev, 2e-3)
+            gpu.kick_drift(ev, 2e-3)
+        out.append(gpu.read_evolving_state_records(ev)[0].tobytes())
+        tree.close()
+        ev.close()
+    assert out[0] == out[1]
+
+
 def test_packed_path_matches_models(gpu, oracle):
     bodies = oracle.make_disc(3000, 303, 5.0e10, 3.0)
     oc = oracle.Config()
