@@ -680,7 +680,8 @@ def run_engine(args, world, rank, local, pg):
             summary["served_at_200_per_s"] = {
                 "requests": spec["requests"], "completed": spec["completed"],
                 "p50_s": r4(spec["p50_s"]), "p99_s": r4(spec["p99_s"]),
-                "value": r4(spec["particle_steps_per_s"]), "busy_frac": r4(spec.get("busy_frac"))}
+                "value": r4(spec["particle_steps_per_s"]), "busy_frac": r4(spec.get("busy_frac")),
+                "thread_seconds": spec.get("thread_seconds")}
     # long objects first, the contract keys and the compact summary last
     # (the end of the line is what a log tail keeps)
     line = {
@@ -992,9 +993,14 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
                 "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
                 "wall_s": wall, "busy_s": st["busy_seconds"], "rounds": st["rounds"],
-                # share of the serving thread's elapsed time spent in rounds
-                "busy_frac": st["busy_seconds"] / st["elapsed_seconds"]
-                if st["elapsed_seconds"] > 0 else None,
+                # share of the serving thread's working time (rounds, admission,
+                # boundary solves, batch re-formation, readback) spent in rounds
+                "busy_frac": st["busy_seconds"] / max(1e-9, sum(
+                    st[k] for k in ("busy_seconds", "admit_seconds", "solve_seconds",
+                                    "form_seconds", "readback_seconds"))),
+                "thread_seconds": {k[:-8]: round(st[k], 3) for k in
+                                   ("busy_seconds", "admit_seconds", "solve_seconds",
+                                    "form_seconds", "readback_seconds", "elapsed_seconds")},
                 "particle_steps": ps, "particle_steps_per_s": ps / wall if wall > 0 else 0.0,
                 "server": "native (galaxy_bh_serve_*)"}
 

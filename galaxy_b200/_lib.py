@@ -97,7 +97,9 @@ class BhServeResult(C.Structure):
 class BhServeStats(C.Structure):
     _fields_ = [("rounds", C.c_uint64), ("particle_steps", C.c_uint64),
                 ("completed", C.c_uint64), ("busy_seconds", C.c_double),
-                ("elapsed_seconds", C.c_double)]
+                ("elapsed_seconds", C.c_double), ("admit_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("form_seconds", C.c_double),
+                ("readback_seconds", C.c_double)]
 
 
 class BhForceStats(C.Structure):

@@ -55,6 +55,7 @@ struct bh_server {
     uint64_t next_id = 1;
     uint64_t rounds = 0, particle_steps = 0, completed = 0;
     double busy_s = 0.0;
+    double admit_s = 0.0, solve_s = 0.0, form_s = 0.0, readback_s = 0.0;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 };
@@ -120,6 +121,7 @@ void serve_loop(bh_server* s) {
         // newcomers are appended after the members already stepping
         const size_t stepping = active.size();
         bool joined = false;
+        const double ta = s->now();
         while (!waiting.empty() && active.size() < s->sc.max_members) {
             std::unique_ptr<ServeRequest>& cand = waiting.front();
             std::vector<uint32_t> counts;
@@ -153,6 +155,11 @@ void serve_loop(bh_server* s) {
             active.push_back(std::move(r));
             joined = true;
         }
+        const double tj = s->now();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->admit_s += tj - ta;
+        }
         if (active.empty()) continue;
         if (joined) {
             // the newcomers need their boundary acceleration (a batch of them
@@ -160,7 +167,13 @@ void serve_loop(bh_server* s) {
             // the members already stepping hold theirs
             int rc = form_batch(s, active, &batch, stepping);
             if (rc == BH_OK) rc = galaxy_bh_batch_solve(s->dev, batch);
+            const double ts = s->now();
             if (rc == BH_OK) rc = form_batch(s, active, &batch);
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->solve_s += ts - tj;
+                s->form_s += s->now() - ts;
+            }
             if (rc != BH_OK) {
                 fail_all_active(rc);
                 continue;
@@ -188,6 +201,7 @@ void serve_loop(bh_server* s) {
         }
         std::vector<std::unique_ptr<ServeRequest>> still;
         bool left = false;
+        const double tr = s->now();
         for (auto& r : active) {
             r->remaining -= r_steps;
             if (r->remaining == 0) {
@@ -201,10 +215,16 @@ void serve_loop(bh_server* s) {
             }
         }
         active = std::move(still);
+        const double tf = s->now();
         if (left) {
             // re-formed batches step at once: every member's acceleration
             // buffer holds its boundary acceleration
             if ((rc = form_batch(s, active, &batch)) != BH_OK) fail_all_active(rc);
+        }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->readback_s += tf - tr;
+            s->form_s += s->now() - tf;
         }
     }
     if (batch) galaxy_bh_batch_destroy(batch);
@@ -305,6 +325,10 @@ extern "C" int galaxy_bh_serve_stats(bh_server* s, bh_serve_stats* out) {
     out->completed = s->completed;
     out->busy_seconds = s->busy_s;
     out->elapsed_seconds = s->now();
+    out->admit_seconds = s->admit_s;
+    out->solve_seconds = s->solve_s;
+    out->form_seconds = s->form_s;
+    out->readback_seconds = s->readback_s;
     return BH_OK;
 }
 

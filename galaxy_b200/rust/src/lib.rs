@@ -167,6 +167,10 @@ pub struct BhServeStats {
     pub completed: u64,
     pub busy_seconds: f64,
     pub elapsed_seconds: f64,
+    pub admit_seconds: f64,
+    pub solve_seconds: f64,
+    pub form_seconds: f64,
+    pub readback_seconds: f64,
 }
 
 /// The raw C ABI, one declaration per function of include/galaxy_bh.h.

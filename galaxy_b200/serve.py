@@ -254,14 +254,14 @@ class NativeServer:
         C, _lib = self._C, self._lib
         res = _lib.BhServeResult()
         cap = self._max_n
-        out = np.zeros(max(cap, 1), _lib.EVOLVE_STATE_DTYPE)
+        out = np.empty(max(cap, 1), _lib.EVOLVE_STATE_DTYPE)
         rc = _lib.load().galaxy_bh_serve_poll(self._h, int(timeout_s * 1000), C.byref(res),
                                               _lib.ptr(out), cap)
         if rc == _lib.BH_TIMEOUT:
             return None
         if rc == _lib.BH_INVALID_ARG and res.n > cap:  # sized by another submitter
             cap = res.n
-            out = np.zeros(cap, _lib.EVOLVE_STATE_DTYPE)
+            out = np.empty(cap, _lib.EVOLVE_STATE_DTYPE)
             rc = _lib.load().galaxy_bh_serve_poll(self._h, 0, C.byref(res), _lib.ptr(out), cap)
         _lib.check(rc)
         info = {"request_id": res.request_id, "n": res.n, "status": res.status,
@@ -275,7 +275,9 @@ class NativeServer:
         _lib.check(_lib.load().galaxy_bh_serve_stats(self._h, C.byref(st)))
         return {"rounds": st.rounds, "particle_steps": st.particle_steps,
                 "completed": st.completed, "busy_seconds": st.busy_seconds,
-                "elapsed_seconds": st.elapsed_seconds}
+                "elapsed_seconds": st.elapsed_seconds, "admit_seconds": st.admit_seconds,
+                "solve_seconds": st.solve_seconds, "form_seconds": st.form_seconds,
+                "readback_seconds": st.readback_seconds}
 
     def stop(self) -> None:
         """Ends the loop and joins its thread; always call it (or use the

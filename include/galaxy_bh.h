@@ -346,9 +346,14 @@ typedef struct {
     uint32_t reserved;
     double submitted_s, admitted_s, finished_s;  /* seconds since serve_start */
 } bh_serve_result;
+/* busy_seconds: rounds of steps; the serving thread's other time splits into
+ * admit (state uploads and checks), solve (newcomers' boundary solves),
+ * form (batch re-formation) and readback (finished results); elapsed is the
+ * time since serve_start. */
 typedef struct {
     uint64_t rounds, particle_steps, completed;
     double busy_seconds, elapsed_seconds;
+    double admit_seconds, solve_seconds, form_seconds, readback_seconds;
 } bh_serve_stats;
 int galaxy_bh_serve_start(int ordinal, const bh_serve_config* config, bh_server** out);
 int galaxy_bh_serve_submit(bh_server* server, const GpuEvolveState* host, uint32_t n,
