@@ -39,7 +39,7 @@ METRIC = "particle-steps/s"
 # Morton, 4 radix passes, count/scan, cells and aggregate for one step at
 # N=2^20, from one capture of this bench's workload; re-measured whenever one
 # of those kernels changes
-BUILD_DRAM_BYTES_PER_STEP = 469.5e6
+BUILD_DRAM_BYTES_PER_STEP = 456.2e6
 WORKLOAD = "cold-collapse uniform disc N=2^20, eps=0.005, theta=0.5, bucket=1, dt=5e-4, seed 7"
 
 def algorithmic_bytes(c: float) -> dict:
@@ -505,6 +505,19 @@ def run_engine(args, world, rank, local, pg):
     if pg:
         pg.barrier()
     value = world * N_BODIES * args.steps / (ms * 1e-3)
+    if args.only_step:
+        # the timed steps alone (for profilers: no other leg launches a kernel)
+        tree.close()
+        ev.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": METRIC,
+                              "n_gpus": world, "steps": args.steps,
+                              "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps,
+                              "only_step": True, "config": config_dict(world)}), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
 
     # --- spread: the same steps as 10 shorter timed runs, p50/p99 per step
     rep_steps, rep_ms = 20, []
@@ -1099,6 +1112,9 @@ def main():
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the precision-form leg (binary encounter, N=2^22)")
     ap.add_argument("--precision-steps", type=int, default=500)
+    ap.add_argument("--only-step", action="store_true",
+                    help="run the timed steps of the headline workload and nothing else "
+                         "(a short line without the side legs; for profilers)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":

@@ -203,7 +203,8 @@ constexpr long long kSpinCycles = 2000000000ll;
 #ifndef GBH_INTEGRATE_UNROLL
 #define GBH_INTEGRATE_UNROLL 4
 #endif
-constexpr int kIntegrateUnroll = GBH_INTEGRATE_UNROLL;  // chunks whose loads a warp keeps in flight
+// chunks whose loads a warp keeps in flight (modes with the bounds reduction)
+constexpr int kIntegrateUnrollBounds = GBH_INTEGRATE_UNROLL;
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ sims,
@@ -211,6 +212,9 @@ __global__ void __launch_bounds__(256) k_integrate(const SimDesc* __restrict__ s
                                                    uint32_t nchunks, uint32_t* minmax) {
     wait_for_predecessor();
     constexpr bool kBounds = MODE != 2;
+    // without the bounds reduction (no atomics) one warp per chunk streams
+    // best; with it, fewer blocks each keeping several chunks' loads in flight
+    constexpr int kIntegrateUnroll = kBounds ? kIntegrateUnrollBounds : 1;
     __shared__ uint32_t s_sim[8];
     __shared__ float s_val[8][4];
     const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
@@ -1963,7 +1967,8 @@ static uint32_t integrate_blocks(uint32_t nchunks) {
 #ifdef GBH_INTEGRATE_BLOCKS_PER_SM
     const uint32_t cap = (uint32_t)(sm_count() * GBH_INTEGRATE_BLOCKS_PER_SM);
 #else
-    const uint32_t cap = (uint32_t)(sm_count() * r);
+    // the final kick (no bounds atomics): one warp per chunk
+    const uint32_t cap = MODE == 2 ? 0xffffffffu : (uint32_t)(sm_count() * r);
 #endif
     const uint32_t blocks = (nchunks + 7) / 8;
     return blocks < cap ? (blocks ? blocks : 1u) : cap;
