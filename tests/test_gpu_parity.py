@@ -204,6 +204,31 @@ def test_kick_drift_final_kick_bit_exact(gpu, oracle):
         np.testing.assert_allclose(r, want, rtol=5e-7, atol=2e-9)
 
 
+def test_force_f64_checks_its_arguments(gpu, rt):
+    """galaxy_bh_force_f64 needs a rebuilt tree and an output buffer, and
+    leaves the state's f32 accelerations as they were."""
+    import ctypes as C
+
+    from galaxy_b200 import _lib
+    cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
+    ev, _ = gpu.create_evolving_state(scenarios.cold_disc(5000, 2))
+    tree = rt.create_tree(gpu, ev, cfg)
+    with pytest.raises(_lib.EngineError, match="rebuilt tree"):
+        rt.force_f64(gpu, ev, tree, cfg)
+    rt.rebuild(gpu, ev, tree, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    before, _ = gpu.read_evolving_accelerations_f32(ev)
+    L = _lib.load()
+    assert L.galaxy_bh_force_f64(gpu.handle, ev.handle, tree.handle, C.byref(cfg.to_c()), None,
+                                 None, None) == _lib.BH_INVALID_ARG
+    acc, s, st = rt.force_f64(gpu, ev, tree, cfg, abs_sum=True)
+    after, _ = gpu.read_evolving_accelerations_f32(ev)
+    assert np.array_equal(before.view(np.uint32), after.view(np.uint32))
+    assert np.isfinite(acc).all() and (s > 0).all() and st["visited_nodes"] > 0
+    tree.close()
+    ev.close()
+
+
 def test_final_kick_drift_equals_the_two_calls(gpu, rt):
     """galaxy_bh_final_kick_drift (one pass) leaves the records bit-identical
     to galaxy_bh_final_kick followed by galaxy_bh_kick_drift."""

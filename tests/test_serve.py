@@ -220,3 +220,39 @@ def test_native_server_results_equal_alone():
         rt.step(gpu, ev, tree, cfg, 1e-3, steps)
         alone, _ = gpu.read_evolving_state_records(ev)
         assert np.array_equal(alone.view(np.uint32), results[k].view(np.uint32)), name
+
+
+@pytest.mark.gpu
+def test_native_server_stop_releases_a_waiting_poll():
+    """stop ends the loop while a request is still stepping and a poll is
+    waiting in another thread: the poll returns "server stopped", stop
+    returns, and nothing waits for the dropped request."""
+    import threading
+    import time
+
+    from galaxy_b200 import _lib, scenarios
+    from galaxy_b200._lib import EngineError
+    from galaxy_b200.nbody_gpu import Config, bodies_to_state
+    from galaxy_b200.serve import NativeServer
+
+    srv = NativeServer(0, budget_bytes=8 << 30, round_steps=2)
+    srv.submit(bodies_to_state(scenarios.make("cold_disc", 200000, 3)),
+               Config(theta=0.5, softening_kpc=0.01, g=1.0), 1e-3, 100000)
+    out = {}
+
+    def waiter():
+        try:
+            out["result"] = srv.poll(timeout_s=60.0)
+        except EngineError as e:
+            out["error"] = e
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    time.sleep(0.5)
+    t0 = time.perf_counter()
+    srv.stop()
+    th.join(timeout=20.0)
+    assert not th.is_alive()
+    assert time.perf_counter() - t0 < 20.0
+    assert "error" in out, out
+    assert out["error"].status == _lib.BH_INVALID_ARG and "stopped" in out["error"].message

@@ -110,6 +110,15 @@ def test_noalloc_at_the_limit_allocates_nothing():
         return d_sums.cpu().numpy()
 
     first = call()
+    # on a stream of the caller's own, too
+    side = torch.cuda.Stream()
+    d_side = torch.full((9,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()  # the side stream is not ordered after the fill
+    _lib.check(lib.galaxy_bh_conservation_noalloc(
+        C.c_void_p(d_state.data_ptr()), None, n, C.c_void_p(d_side.data_ptr()),
+        C.c_void_p(side.cuda_stream)))
+    side.synchronize()
+    assert np.array_equal(d_side.cpu().numpy(), first)
     free_before, _ = torch.cuda.mem_get_info()
     second = call()
     free_after, _ = torch.cuda.mem_get_info()
