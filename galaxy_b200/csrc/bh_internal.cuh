@@ -17,7 +17,7 @@ constexpr uint32_t kTile = kSortThreads * kSortItems;  // keys per radix tile (4
 constexpr int kRadixDigits = 256;
 constexpr int kRadixPasses = 4;
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 4;  // 1024-position scan tiles: a shorter per-tile chain
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // positions per scan tile
 constexpr uint32_t kMortonDepth = 16;
 

@@ -153,6 +153,59 @@ __device__ __forceinline__ uint32_t gallop_lower_bound(const uint32_t* codes, ui
     return lo;
 }
 
+// First index in [lo, hi) whose code is >= x (codes ascending there; hi if
+// none), for NT targets at once, by 8-way partition: each round loads seven
+// evenly spaced codes per unfinished target — all of them one round trip —
+// and keeps the eighth of the range that holds the bound; the last <= 8
+// positions are counted with independent loads.  A range of D positions
+// takes log8(D) + 1 round trips instead of the ~2 log2(D) dependent loads of
+// a binary search, which is what the few cells spanning most of the
+// positions (near the root) wait for.
+template <int NT>
+__device__ __forceinline__ void kary_lower_bound(const uint32_t* codes, uint32_t lo, uint32_t hi,
+                                                 const uint32_t (&x)[NT], uint32_t (&out)[NT]) {
+    uint32_t l[NT], h[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        l[t] = lo;
+        h[t] = hi;
+    }
+    while (true) {
+        bool more = false;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) more = more || h[t] - l[t] > 8u;
+        if (!more) break;
+        uint32_t c[NT][7];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const uint32_t step = (h[t] - l[t]) / 8u;
+#pragma unroll
+            for (int j = 0; j < 7; ++j)
+                c[t][j] = step ? __ldg(codes + l[t] + step * (uint32_t)(j + 1)) : 0u;
+        }
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const uint32_t step = (h[t] - l[t]) / 8u;
+            if (!step) continue;
+            uint32_t below = 0;  // probes below x: the probes are ascending
+#pragma unroll
+            for (int j = 0; j < 7; ++j) below += c[t][j] < x[t] ? 1u : 0u;
+            const uint32_t nl = below ? l[t] + step * below + 1u : l[t];
+            const uint32_t nh = below < 7u ? l[t] + step * (below + 1u) : h[t];
+            l[t] = nl;
+            h[t] = nh;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+        uint32_t below = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            below += (l[t] + (uint32_t)j < h[t] && __ldg(codes + l[t] + j) < x[t]) ? 1u : 0u;
+        out[t] = l[t] + below;
+    }
+}
+
 // Exclusive scan over a 256-thread block; *total gets the block sum.
 __device__ __forceinline__ uint32_t block_exclusive_scan_256(uint32_t v, uint32_t* total,
                                                              uint32_t* smem8) {
@@ -391,8 +444,14 @@ constexpr uint32_t kHistStride = kRadixPasses * kRadixDigits;  // histogram word
 // One block per radix tile: Morton codes of the tile's bodies (resident
 // order) plus the tile's contribution to the digit histograms of every pass
 // of a BITS-wide LSD sort (hist[sim][pass * 2^BITS + digit]).
+// Threads per Morton block (one radix tile of kTile keys): 512 hide more of
+// the quantization's f64 latency than 256 (and than 1024).
+constexpr int kMortonThreads = 512;
+constexpr int kMortonItems = (int)kTile / kMortonThreads;
+static_assert(kMortonItems * kMortonThreads == (int)kTile, "a Morton block covers one tile");
+
 template <int BITS>
-__global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restrict__ sims,
+__global__ void __launch_bounds__(kMortonThreads) k_morton(const SimDesc* __restrict__ sims,
                                                          const Tile* __restrict__ tiles,
                                                          const uint32_t* __restrict__ minmax,
                                                          uint32_t* __restrict__ keys,
@@ -401,7 +460,7 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
     constexpr int kPasses = 32 / BITS;
     constexpr uint32_t kDig = 1u << BITS;
     __shared__ uint32_t sh[kPasses * kDig];
-    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kSortThreads) sh[k] = 0;
+    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kMortonThreads) sh[k] = 0;
     __syncthreads();
     const Tile t = tiles[blockIdx.x];
     const SimDesc& sd = sims[t.sim];
@@ -412,8 +471,8 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
         simout[t.sim].half = rb.half;
     }
 #pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const uint32_t idx = k * kSortThreads + threadIdx.x;
+    for (int k = 0; k < kMortonItems; ++k) {
+        const uint32_t idx = k * kMortonThreads + threadIdx.x;
         if (idx < t.count) {
             const uint32_t p = t.start + idx;
             const float2 xy = *reinterpret_cast<const float2*>(sd.state + (p - sd.off));
@@ -426,7 +485,7 @@ __global__ void __launch_bounds__(kSortThreads) k_morton(const SimDesc* __restri
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kSortThreads) {
+    for (int k = threadIdx.x; k < kPasses * (int)kDig; k += kMortonThreads) {
         const uint32_t c = sh[k];
         if (c) atomicAdd(&hist[(size_t)t.sim * kHistStride + k], c);
     }
@@ -746,6 +805,10 @@ constexpr uint32_t kCellsThreads = 256;
 constexpr uint32_t kCellsWin = 1024;
 constexpr uint32_t kMaxChain = kMortonDepth + 1;  // cells per position: depths 0..16
 
+#ifndef GBH_CELLS_KARY
+#define GBH_CELLS_KARY 1
+#endif
+
 struct CellsWindow {
     const uint32_t* s_code;  // codes of positions [w0, w0 + kCellsWin)
     const uint32_t* s_base;  // base of positions [w0, w0 + kCellsWin]
@@ -766,11 +829,62 @@ struct CellsWindow {
                 return w0 + gallop_lower_bound(s_code, lo - w0, wend - w0, x);
             lo = wend;
         }
+#if GBH_CELLS_KARY
+        if (lo >= hi) return hi;
+        const uint32_t xs[1] = {x};
+        uint32_t r[1];
+        kary_lower_bound<1>(codes, lo, hi, xs, r);
+        return r[0];
+#else
         return lo < hi ? gallop_lower_bound(codes, lo, hi, x) : hi;
+#endif
+    }
+    // The three quadrant bounds of a cell's range [lo, hi): out[q] = first
+    // position whose code is >= x[q] (x ascending), the window first, the
+    // searches past it together.
+    __device__ __forceinline__ void lower_bound3(uint32_t lo, uint32_t hi, const uint32_t (&x)[3],
+                                                 uint32_t (&out)[3]) const {
+#if GBH_CELLS_KARY
+        const uint32_t wend = min(hi, w0 + kCellsWin);
+        bool far = false;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if (lo < wend && s_code[wend - 1u - w0] >= x[q]) {
+                out[q] = w0 + gallop_lower_bound(s_code, lo - w0, wend - w0, x[q]);
+            } else {
+                out[q] = kNone;
+                far = true;
+            }
+        }
+        if (far) {
+            const uint32_t flo = max(lo, wend);
+            uint32_t r[3];
+            if (flo < hi) {
+                kary_lower_bound<3>(codes, flo, hi, x, r);
+            } else {
+                r[0] = r[1] = r[2] = hi;
+            }
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (out[q] == kNone) out[q] = r[q];
+        }
+#else
+        uint32_t l = lo;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            l = lower_bound(l, hi, x[q]);
+            out[q] = l;
+        }
+#endif
     }
 };
 
-__global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restrict__ sims,
+// six blocks per SM (40 registers): the k-ary searches spill a little in
+// the few threads that run them instead of halving every block's occupancy
+#ifndef GBH_CELLS_MIN_BLOCKS
+#define GBH_CELLS_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kCellsThreads, GBH_CELLS_MIN_BLOCKS) k_cells(const SimDesc* __restrict__ sims,
                                                          const uint32_t* __restrict__ chunk_sim,
                                                          uint32_t npos, uint32_t capacity,
                                                          const uint32_t* __restrict__ codes,
@@ -873,14 +987,15 @@ __global__ void __launch_bounds__(kCellsThreads) k_cells(const SimDesc* __restri
             }
             if (searched) {
                 const uint32_t pre = d == 0 ? 0u : (s_code[p - P0] >> (32u - 2u * d));
+                const uint32_t xs[3] = {((pre << 2) | 1u) << sh, ((pre << 2) | 2u) << sh,
+                                        ((pre << 2) | 3u) << sh};
+                uint32_t qb[3];
+                w.lower_bound3(p, end, xs, qb);
                 uint32_t bounds[5];
                 bounds[0] = p;
-                uint32_t lo = p;
-#pragma unroll
-                for (uint32_t qd = 1; qd < 4; ++qd) {
-                    lo = w.lower_bound(lo, end, ((pre << 2) | qd) << sh);
-                    bounds[qd] = lo;
-                }
+                bounds[1] = qb[0];
+                bounds[2] = qb[1];
+                bounds[3] = qb[2];
                 bounds[4] = end;
 #pragma unroll
                 for (uint32_t qd = 0; qd < 4; ++qd)
@@ -1139,8 +1254,11 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
         const bool right = sd.off + sd.n <= P1 || shared_levels(c, s_code[P1 - P0 + 1u]) < dd;
         return left && right;
     };
+    // the next cell's links are loaded while this one is summed
+    uint4 u_next = kb + t < ke ? a.cell_u[kb + t] : make_uint4(0u, 0u, 0u, 0u);
     for (uint32_t k = kb + t; k < ke; k += kAggThreads) {
-        const uint4 u = a.cell_u[k];  // (end, skip, start, depth)
+        const uint4 u = u_next;  // (end, skip, start, depth)
+        if (k + kAggThreads < ke) u_next = a.cell_u[k + kAggThreads];
         const SimDesc& sd = a.sims[a.chunk_sim[u.z >> 5]];
         if (u.y == k + 1u) {
             aggregate_cell(a, k, u, true);
@@ -1986,9 +2104,9 @@ cudaError_t launch_integrate(const BatchBuffers& b, int mode, cudaStream_t s) {
 
 cudaError_t launch_morton(const BatchBuffers& b, cudaStream_t s) {
     if (b.radix_bits == 4)
-        return launch_step(k_morton<4>, b.ntiles, kSortThreads, 0, s, b.sims, b.tiles, b.minmax,
+        return launch_step(k_morton<4>, b.ntiles, kMortonThreads, 0, s, b.sims, b.tiles, b.minmax,
                            b.keys_a, b.hist, b.simout);
-    return launch_step(k_morton<8>, b.ntiles, kSortThreads, 0, s, b.sims, b.tiles, b.minmax,
+    return launch_step(k_morton<8>, b.ntiles, kMortonThreads, 0, s, b.sims, b.tiles, b.minmax,
                        b.keys_a, b.hist, b.simout);
 }
 
