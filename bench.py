@@ -39,7 +39,7 @@ METRIC = "particle-steps/s"
 # Morton, 4 radix passes, count/scan, cells and aggregate for one step at
 # N=2^20, from one capture of this bench's workload; re-measured whenever one
 # of those kernels changes
-BUILD_DRAM_BYTES_PER_STEP = 456.2e6
+BUILD_DRAM_BYTES_PER_STEP = 465.5e6
 WORKLOAD = "cold-collapse uniform disc N=2^20, eps=0.005, theta=0.5, bucket=1, dt=5e-4, seed 7"
 
 def algorithmic_bytes(c: float) -> dict:
