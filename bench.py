@@ -1006,11 +1006,11 @@ def run_served_leg(gpu, capacity: float, duration: float = 20.0, budget_gb: floa
                 "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
                 "wall_s": wall, "busy_s": st["busy_seconds"], "rounds": st["rounds"],
-                # share of the serving thread's working time (rounds, admission,
-                # boundary solves, batch re-formation, readback) spent in rounds
+                # share of the serving thread's working time (rounds, batch
+                # re-formation, readback) spent in rounds; admission and
+                # boundary solves run on the stager thread, overlapping them
                 "busy_frac": st["busy_seconds"] / max(1e-9, sum(
-                    st[k] for k in ("busy_seconds", "admit_seconds", "solve_seconds",
-                                    "form_seconds", "readback_seconds"))),
+                    st[k] for k in ("busy_seconds", "form_seconds", "readback_seconds"))),
                 "thread_seconds": {k[:-8]: round(st[k], 3) for k in
                                    ("busy_seconds", "admit_seconds", "solve_seconds",
                                     "form_seconds", "readback_seconds", "elapsed_seconds")},

@@ -73,22 +73,17 @@ struct bh_device {
     cudaDeviceProp prop{};
     int refs = 0;         // live states, trees and batches on this device
     bool closed = false;  // galaxy_bh_device_close was called
-    // One released batch arena kept for the next batch: a serving loop that
-    // re-forms its batch after every membership change reuses it instead of
-    // freeing and allocating gigabytes each time.
-    void* spare = nullptr;
-    size_t spare_bytes = 0;
-    // Stream-ordered pool of the per-state buffers.  It keeps released
-    // memory for the next state (trimmed only when an arena allocation runs
-    // short): cudaFree synchronizes the device and unmaps pages, which cost
-    // a serving loop seconds per burst of finished requests.
+    // Stream-ordered pool of the per-state buffers and the batch / tree
+    // arenas.  It keeps released memory for reuse (trimmed only when an
+    // arena allocation runs short): cudaFree synchronizes the whole device
+    // and unmaps pages, which cost a serving loop seconds per burst of
+    // finished requests and would stall it on its stager's work.
     cudaMemPool_t pool = nullptr;
 };
 
 static void device_free(bh_device* dev) {
     cudaSetDevice(dev->ordinal);
     cudaStreamSynchronize(dev->stream);
-    cudaFree(dev->spare);
     if (dev->pool) cudaMemPoolDestroy(dev->pool);
     for (auto& ev : dev->ev) cudaEventDestroy(ev);
     cudaStreamDestroy(dev->stream);
@@ -319,12 +314,30 @@ extern "C" int galaxy_bh_state_destroy(bh_state* st) {
                         (void*)st->d_chunk_sim, (void*)st->d_minmax, (void*)st->d_check})
             if (p) cudaFreeAsync(p, st->dev->stream);
     }
-    cudaFree(st->d_potential);
-    cudaFree(st->d_cons);
-    cudaFree(st->d_stage);
+    if (st->d_potential) cudaFree(st->d_potential);
+    if (st->d_cons) cudaFree(st->d_cons);
+    if (st->d_stage) cudaFree(st->d_stage);
     bh_device* dev = st->dev;
     delete st;
     device_unref(dev);
+    return BH_OK;
+}
+
+// Hands a state made on one device handle to another handle of the same
+// GPU (the serving loop's stager uploads and solves on its own handle and
+// stream): the state's pending work finishes first; its buffers stay where
+// they are and are later released on the new handle's stream.
+int gbh::state_move(bh_state* st, bh_device* to) {
+    if (!st || !to) return set_error(BH_INVALID_ARG, "null argument");
+    if (st->dev == to) return BH_OK;
+    if (st->dev->ordinal != to->ordinal)
+        return set_error(BH_INVALID_ARG, "state and device handle are on different GPUs");
+    CK(cudaSetDevice(st->dev->ordinal), "cudaSetDevice");
+    CK(cudaStreamSynchronize(st->dev->stream), "state move");
+    bh_device* old = st->dev;
+    device_ref(to);
+    st->dev = to;
+    device_unref(old);
     return BH_OK;
 }
 
@@ -574,21 +587,15 @@ struct Batch {
     // (single-simulation trees; batches keep their creation configs)
     double built_theta = NAN, built_g = NAN;
 
-    size_t arena_capacity = 0;  // bytes actually held (>= arena_bytes when reused)
+    size_t arena_capacity = 0;  // bytes held
 
     ~Batch() {
         for (auto& g : graphs)
             if (g) cudaGraphExecDestroy(g);
-        if (!arena) return;
-        // keep the larger of this arena and the device's spare
-        cudaStreamSynchronize(dev->stream);
-        if (arena_capacity > dev->spare_bytes) {
-            cudaFree(dev->spare);
-            dev->spare = arena;
-            dev->spare_bytes = arena_capacity;
-        } else {
-            cudaFree(arena);
-        }
+        // back to the device handle's pool in stream order: no device-wide
+        // synchronisation (a cudaFree would wait for every stream of the GPU,
+        // e.g. a serving loop's rounds while its stager releases a tree)
+        if (arena) cudaFreeAsync(arena, dev->stream);
     }
 };
 
@@ -690,26 +697,17 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     b->cell_capacity = L.cells;
     b->arena_bytes = A.total();
     cudaError_t e = cudaSuccess;
-    if (dev->spare && dev->spare_bytes >= b->arena_bytes) {
-        b->arena = dev->spare;  // reuse the released arena of an earlier batch
-        b->arena_capacity = dev->spare_bytes;
-        dev->spare = nullptr;
-        dev->spare_bytes = 0;
-    } else {
+    // the arena comes from the device handle's stream-ordered pool, which
+    // keeps released arenas and state buffers for reuse
+    e = cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, dev->pool, dev->stream);
+    if (e == cudaErrorMemoryAllocation) {
+        // give back what the pool keeps, then retry
+        cudaGetLastError();
         cudaStreamSynchronize(dev->stream);
-        cudaFree(dev->spare);  // too small: give its memory back first
-        dev->spare = nullptr;
-        dev->spare_bytes = 0;
-        e = cudaMalloc(&b->arena, b->arena_bytes);
-        if (e == cudaErrorMemoryAllocation) {
-            // give back the released state memory the pool keeps, then retry
-            cudaGetLastError();
-            cudaStreamSynchronize(dev->stream);
-            cudaMemPoolTrimTo(dev->pool, 0);
-            e = cudaMalloc(&b->arena, b->arena_bytes);
-        }
-        b->arena_capacity = b->arena_bytes;
+        cudaMemPoolTrimTo(dev->pool, 0);
+        e = cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, dev->pool, dev->stream);
     }
+    b->arena_capacity = b->arena_bytes;
     if (e != cudaSuccess) {
         b->arena = nullptr;
         delete b;

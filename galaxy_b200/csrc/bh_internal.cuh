@@ -163,6 +163,10 @@ uint32_t conservation_blocks(uint32_t n);
 cudaError_t launch_check_records(const void* records, int kind, uint32_t n, uint32_t* first_bad,
                                  cudaStream_t s);
 
+// Hands state st (made on another handle of the same GPU) to device handle
+// `to`, after the state's pending work (bh_engine.cu).
+int state_move(bh_state* st, bh_device* to);
+
 // Sets the calling thread's last-error message (bh_engine.cu); returns status.
 int set_error_message(int status, const char* message);
 

@@ -43,13 +43,20 @@ struct ServeRequest {
 }  // namespace
 
 struct bh_server {
-    bh_device* dev = nullptr;
+    bh_device* dev = nullptr;    // the serving loop's handle: rounds of steps
+    bh_device* dev2 = nullptr;   // the stager's handle: uploads and boundary solves
     bh_serve_config sc{};
     Clock::time_point t0;
-    std::thread loop;
+    std::thread loop, stager;
     std::mutex mu;
-    std::condition_variable cv_in, cv_out;
-    std::deque<std::unique_ptr<ServeRequest>> submitted, done;
+    std::condition_variable cv_in, cv_out, cv_stage;
+    // submitted -> (stager: state uploaded, checked, boundary-solved) staged
+    // -> (loop) active -> done
+    std::deque<std::unique_ptr<ServeRequest>> submitted, staged, done;
+    // the active members' sizes and configs, published by the loop for the
+    // stager's budget check
+    std::vector<uint32_t> active_n;
+    std::vector<bh_config> active_cfg;
     bool stopping = false;
     int pollers = 0;  // polls inside galaxy_bh_serve_poll (stop waits for them)
     uint64_t next_id = 1;
@@ -89,10 +96,123 @@ int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active,
     return galaxy_bh_batch_create(s->dev, states.data(), cfgs.data(), (uint32_t)states.size(), b);
 }
 
+// Whether `cand` joins the active members and the staged requests inside
+// the budget (caller holds s->mu); *alone_too_big when it can never fit.
+bool fits_budget(bh_server* s, const ServeRequest& cand, bool* alone_too_big) {
+    std::vector<uint32_t> counts(s->active_n);
+    std::vector<bh_config> cfgs(s->active_cfg);
+    for (auto& r : s->staged) {
+        counts.push_back(r->n);
+        cfgs.push_back(r->cfg);
+    }
+    counts.push_back(cand.n);
+    cfgs.push_back(cand.cfg);
+    uint64_t bytes = 0, alone = 0;
+    *alone_too_big = false;
+    if (galaxy_bh_batch_footprint(counts.data(), cfgs.data(), (uint32_t)counts.size(), &bytes) !=
+        BH_OK)
+        return false;
+    if (bytes <= s->sc.budget_bytes) return true;
+    if (galaxy_bh_batch_footprint(&cand.n, &cand.cfg, 1, &alone) == BH_OK &&
+        alone > s->sc.budget_bytes)
+        *alone_too_big = true;
+    return false;
+}
+
+constexpr size_t kStageAhead = 4;  // requests the stager prepares ahead of admission
+
+// The stager: in arrival order, for the requests that fit the budget next to
+// the active and the already staged ones, uploads and checks the initial
+// state and runs its boundary solve (rebuild + force, a tree of its own) on
+// the stager's handle and stream, so that this host work and its copies
+// overlap the rounds the loop keeps running; then hands the state to the
+// loop's handle.  A simulation's result does not depend on where its solve
+// ran: the tree kernels are the same.
+void stage_loop(bh_server* s) {
+    // pinned staging of the records: an upload from pageable memory goes
+    // through the driver's shared bounce buffers, which would hold up the
+    // serving loop's own small uploads behind this one
+    GpuEvolveState* pinned = nullptr;
+    size_t pinned_n = 0;
+    while (true) {
+        std::unique_ptr<ServeRequest> r;
+        int rc = BH_OK;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            bool too_big = false;
+            s->cv_stage.wait(lk, [&] {
+                return s->stopping ||
+                       (!s->submitted.empty() && s->staged.size() < kStageAhead &&
+                        (fits_budget(s, *s->submitted.front(), &too_big) || too_big));
+            });
+            if (s->stopping) break;
+            r = std::move(s->submitted.front());
+            s->submitted.pop_front();
+            if (too_big) rc = BH_CAPACITY_OVERFLOW;  // alone it can never fit
+        }
+        const double t0 = s->now();
+        const GpuEvolveState* src = r->records.data();
+        if (rc == BH_OK) {
+            if (pinned_n < r->n) {
+                if (pinned) cudaFreeHost(pinned);
+                pinned = nullptr;
+                pinned_n = 0;
+                if (cudaMallocHost((void**)&pinned, sizeof(GpuEvolveState) * (size_t)r->n) ==
+                    cudaSuccess)
+                    pinned_n = r->n;
+                else
+                    cudaGetLastError();  // upload from the pageable copy instead
+            }
+            if (pinned_n >= r->n) {
+                std::memcpy(pinned, src, sizeof(GpuEvolveState) * (size_t)r->n);
+                src = pinned;
+            }
+            rc = galaxy_bh_state_create(s->dev2, src, r->n, &r->st, nullptr);
+        }
+        const double t1 = s->now();
+        if (rc == BH_OK) {
+            bh_tree* tree = nullptr;
+            rc = galaxy_bh_tree_create(s->dev2, r->st, &r->cfg, &tree);
+            if (rc == BH_OK) rc = galaxy_bh_tree_rebuild(s->dev2, r->st, tree, &r->cfg, nullptr);
+            bh_config fc = r->cfg;
+            fc.flags |= BH_FLAG_NO_STATS;
+            if (rc == BH_OK) rc = galaxy_bh_force(s->dev2, r->st, tree, &fc, nullptr);
+            if (tree) galaxy_bh_tree_destroy(tree);
+            if (rc == BH_OK) rc = gbh::state_move(r->st, s->dev);
+        }
+        const double t2 = s->now();
+        if (rc != BH_OK) {
+            release_state(r);
+            r->status = rc;
+            r->finished_s = s->now();
+            finish(s, std::move(r));
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->admit_s += t1 - t0;
+            s->solve_s += t2 - t1;
+            continue;
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->admit_s += t1 - t0;
+        s->solve_s += t2 - t1;
+        s->staged.push_back(std::move(r));
+        s->cv_in.notify_all();
+    }
+    if (pinned) cudaFreeHost(pinned);
+}
+
 void serve_loop(bh_server* s) {
-    std::deque<std::unique_ptr<ServeRequest>> waiting;
     std::vector<std::unique_ptr<ServeRequest>> active;
     bh_batch* batch = nullptr;
+    // publishes the active set for the stager's budget check (caller holds mu)
+    auto publish = [&]() {
+        s->active_n.clear();
+        s->active_cfg.clear();
+        for (auto& r : active) {
+            s->active_n.push_back(r->n);
+            s->active_cfg.push_back(r->cfg);
+        }
+        s->cv_stage.notify_all();
+    };
     auto fail_all_active = [&](int rc) {
         for (auto& r : active) {
             release_state(r);
@@ -103,76 +223,38 @@ void serve_loop(bh_server* s) {
         active.clear();
         if (batch) galaxy_bh_batch_destroy(batch);
         batch = nullptr;
+        std::lock_guard<std::mutex> lk(s->mu);
+        publish();
     };
     while (true) {
+        // admission: staged requests join in arrival order (the stager kept
+        // the active set plus every staged request inside the budget)
+        bool joined = false;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (s->stopping) break;
-            while (!s->submitted.empty()) {
-                waiting.push_back(std::move(s->submitted.front()));
-                s->submitted.pop_front();
-            }
-            if (waiting.empty() && active.empty()) {
+            if (s->staged.empty() && active.empty()) {
                 s->cv_in.wait_for(lk, std::chrono::milliseconds(50));
                 continue;
             }
-        }
-        // admission, in arrival order, against the device-memory budget;
-        // newcomers are appended after the members already stepping
-        const size_t stepping = active.size();
-        bool joined = false;
-        const double ta = s->now();
-        while (!waiting.empty() && active.size() < s->sc.max_members) {
-            std::unique_ptr<ServeRequest>& cand = waiting.front();
-            std::vector<uint32_t> counts;
-            std::vector<bh_config> cfgs;
-            for (auto& r : active) {
-                counts.push_back(r->n);
-                cfgs.push_back(r->cfg);
+            while (!s->staged.empty() && active.size() < s->sc.max_members) {
+                std::unique_ptr<ServeRequest> r = std::move(s->staged.front());
+                s->staged.pop_front();
+                r->admitted_s = s->now();
+                r->remaining = r->steps;
+                active.push_back(std::move(r));
+                joined = true;
             }
-            counts.push_back(cand->n);
-            cfgs.push_back(cand->cfg);
-            uint64_t bytes = 0;
-            int rc = galaxy_bh_batch_footprint(counts.data(), cfgs.data(),
-                                               (uint32_t)counts.size(), &bytes);
-            if (rc == BH_OK && bytes > s->sc.budget_bytes) {
-                if (!active.empty()) break;  // wait for room
-                rc = BH_CAPACITY_OVERFLOW;   // alone it can never fit
-            }
-            if (rc == BH_OK)
-                rc = galaxy_bh_state_create(s->dev, cand->records.data(), cand->n, &cand->st,
-                                            nullptr);
-            std::unique_ptr<ServeRequest> r = std::move(cand);
-            waiting.pop_front();
-            if (rc != BH_OK) {
-                r->status = rc;
-                r->finished_s = s->now();
-                finish(s, std::move(r));
-                continue;
-            }
-            r->admitted_s = s->now();
-            r->remaining = r->steps;
-            active.push_back(std::move(r));
-            joined = true;
+            if (joined) publish();
         }
-        const double tj = s->now();
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->admit_s += tj - ta;
-        }
-        if (active.empty()) continue;
         if (joined) {
-            // the newcomers need their boundary acceleration (a batch of them
-            // alone: members' results do not depend on their batch mates);
-            // the members already stepping hold theirs
-            int rc = form_batch(s, active, &batch, stepping);
-            if (rc == BH_OK) rc = galaxy_bh_batch_solve(s->dev, batch);
-            const double ts = s->now();
-            if (rc == BH_OK) rc = form_batch(s, active, &batch);
+            // every member holds its boundary acceleration: the newcomers'
+            // from their staged solves, the others' from their last step
+            const double tf = s->now();
+            const int rc = form_batch(s, active, &batch);
             {
                 std::lock_guard<std::mutex> lk(s->mu);
-                s->solve_s += ts - tj;
-                s->form_s += s->now() - ts;
+                s->form_s += s->now() - tf;
             }
             if (rc != BH_OK) {
                 fail_all_active(rc);
@@ -217,6 +299,10 @@ void serve_loop(bh_server* s) {
         active = std::move(still);
         const double tf = s->now();
         if (left) {
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                publish();
+            }
             // re-formed batches step at once: every member's acceleration
             // buffer holds its boundary acceleration
             if ((rc = form_batch(s, active, &batch)) != BH_OK) fail_all_active(rc);
@@ -243,13 +329,20 @@ extern "C" int galaxy_bh_serve_start(int ordinal, const bh_serve_config* config,
         return set_error_message(BH_INVALID_ARG,
                                  "serve config needs a budget, round_steps and max_members");
     bh_device* dev = nullptr;
+    bh_device* dev2 = nullptr;
     int rc = galaxy_bh_device_open(ordinal, &dev);
     if (rc != BH_OK) return rc;
+    if ((rc = galaxy_bh_device_open(ordinal, &dev2)) != BH_OK) {
+        galaxy_bh_device_close(dev);
+        return rc;
+    }
     bh_server* s = new bh_server();
     s->dev = dev;
+    s->dev2 = dev2;
     s->sc = *config;
     s->t0 = Clock::now();
     s->loop = std::thread(serve_loop, s);
+    s->stager = std::thread(stage_loop, s);
     *out = s;
     return BH_OK;
 }
@@ -274,6 +367,7 @@ extern "C" int galaxy_bh_serve_submit(bh_server* s, const GpuEvolveState* host, 
     *request_id = r->id;
     s->submitted.push_back(std::move(r));
     s->cv_in.notify_all();
+    s->cv_stage.notify_all();
     return BH_OK;
 }
 
@@ -338,15 +432,20 @@ extern "C" int galaxy_bh_serve_stop(bh_server* s) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stopping = true;
         s->cv_in.notify_all();
+        s->cv_stage.notify_all();
         s->cv_out.notify_all();  // waiting polls return "server stopped"
     }
+    if (s->stager.joinable()) s->stager.join();
     if (s->loop.joinable()) s->loop.join();
+    for (auto& r : s->staged) release_state(r);  // dropped with the unfinished ones
+    s->staged.clear();
     {
         // no poll may still be inside the server when it is freed
         std::unique_lock<std::mutex> lk(s->mu);
         s->cv_out.wait(lk, [&] { return s->pollers == 0; });
     }
     galaxy_bh_device_close(s->dev);
+    galaxy_bh_device_close(s->dev2);
     delete s;
     return BH_OK;
 }

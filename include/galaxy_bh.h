@@ -313,10 +313,13 @@ int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
 
 /* ---- native serving loop --------------------------------------------------
  * No reference counterpart (the reference has no serving path).  A server
- * owns a device handle and one host thread running continuous batching:
- * submitted simulations wait in arrival order, are admitted when the
- * device-memory footprint of the active set plus the newcomer (the
- * galaxy_bh_batch_footprint figure) fits budget_bytes, stay resident, and
+ * owns two device handles of the GPU and two host threads running
+ * continuous batching: submitted simulations are taken in arrival order by
+ * a stager, which, as soon as the device-memory footprint of the active set,
+ * the already staged ones and the newcomer (the galaxy_bh_batch_footprint
+ * figure) fits budget_bytes, uploads and checks the newcomer's state and runs
+ * its boundary solve on its own handle and stream while rounds continue;
+ * the serving loop admits staged simulations, which stay resident and
  * advance together in rounds of at most round_steps fused KDK steps in one
  * batch; a round stops at the smallest remaining step count so finished
  * simulations leave and waiting ones join between rounds.  Each result
@@ -346,10 +349,11 @@ typedef struct {
     uint32_t reserved;
     double submitted_s, admitted_s, finished_s;  /* seconds since serve_start */
 } bh_serve_result;
-/* busy_seconds: rounds of steps; the serving thread's other time splits into
- * admit (state uploads and checks), solve (newcomers' boundary solves),
- * form (batch re-formation) and readback (finished results); elapsed is the
- * time since serve_start. */
+/* busy_seconds: rounds of steps; the serving thread's other working time
+ * splits into form (batch re-formation) and readback (finished results).
+ * admit (state uploads and checks) and solve (boundary solves) are the
+ * stager thread's, on its own device handle and stream, overlapping the
+ * rounds.  elapsed is the time since serve_start. */
 typedef struct {
     uint64_t rounds, particle_steps, completed;
     double busy_seconds, elapsed_seconds;
