@@ -4,7 +4,7 @@
 //
 // A Batch lays one or more simulations out in a shared "position space":
 // simulation s owns positions [off_s, off_s + n_s), off_s a multiple of 32,
-// so a warp never straddles two simulations.  Radix tiles (2048 keys) never
+// so a warp never straddles two simulations.  Radix tiles (4096 keys) never
 // straddle simulations either.  Per-rebuild scratch (keys, sorted bodies,
 // cells, control block) is one device arena carved at batch creation and
 // sized for the worst case, so no step ever allocates.  The plain API
@@ -75,9 +75,9 @@ struct bh_device {
     bool closed = false;  // galaxy_bh_device_close was called
     // Stream-ordered pool of the per-state buffers and the batch / tree
     // arenas.  It keeps released memory for reuse (trimmed only when an
-    // arena allocation runs short): cudaFree synchronizes the whole device
-    // and unmaps pages, which cost a serving loop seconds per burst of
-    // finished requests and would stall it on its stager's work.
+    // allocation runs short): cudaFree synchronizes the whole device and
+    // unmaps pages, which cost a serving loop seconds per burst of finished
+    // requests and would stall it on its stager's work.
     cudaMemPool_t pool = nullptr;
 };
 
@@ -199,11 +199,18 @@ static int validate_config(const bh_config* c) {
 
 static uint32_t eff_depth(const bh_config& c) { return std::min<uint32_t>(c.max_depth, kMortonDepth); }
 
-// Upper bound on cells: leaves are disjoint (<= n); internal cells at one
-// depth hold disjoint ranges of > bucket bodies (<= n/(bucket+1) per depth,
-// depths 0..max_depth-1).
+// Upper bound on cells: leaves are disjoint (<= n); internal cells exist at
+// depths 0..max_depth-1, and those at depth d are at most 4^d (one per
+// quadtree square) and hold disjoint ranges of > bucket bodies (at most
+// n/(bucket+1)).  At bucket 1 this is ~3.8n cells for n = 2^22 (a
+// depth-blind n/(bucket+1) per depth would be 9n); trees of real
+// distributions hold ~1.7n.
 static uint64_t cell_bound(uint32_t n, const bh_config& c) {
-    return (uint64_t)n + (uint64_t)eff_depth(c) * (n / ((uint64_t)c.bucket + 1)) + 1;
+    const uint64_t per_depth = n / ((uint64_t)c.bucket + 1);
+    uint64_t internal = 0, squares = 1;
+    for (uint32_t d = 0; d < eff_depth(c); ++d, squares *= 4)
+        internal += std::min(squares, per_depth);
+    return (uint64_t)n + internal + 1;
 }
 
 static void fill_physics(SimDesc& sd, const bh_config& c) {
@@ -258,7 +265,15 @@ extern "C" int galaxy_bh_state_create(bh_device* dev, const GpuEvolveState* host
     cudaError_t e;
     std::vector<uint32_t> chunk(st->nchunks, 0u);
     auto pool_alloc = [&](auto** ptr, size_t bytes) {
-        return cudaMallocFromPoolAsync((void**)ptr, bytes, dev->pool, dev->stream);
+        cudaError_t r = cudaMallocFromPoolAsync((void**)ptr, bytes, dev->pool, dev->stream);
+        if (r == cudaErrorMemoryAllocation) {
+            // give back what the pool keeps unused, then retry
+            cudaGetLastError();
+            cudaStreamSynchronize(dev->stream);
+            cudaMemPoolTrimTo(dev->pool, 0);
+            r = cudaMallocFromPoolAsync((void**)ptr, bytes, dev->pool, dev->stream);
+        }
+        return r;
     };
     if ((e = pool_alloc(&st->d_state, sizeof(GpuEvolveState) * (size_t)n)) ||
         (e = pool_alloc(&st->d_accel, sizeof(float4) * (size_t)n)) ||

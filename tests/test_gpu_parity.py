@@ -133,6 +133,36 @@ def test_clustered_pairs_hit_depth_limit(gpu, rt, oracle):
         assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
 
 
+def _cell_bound(n, bucket, depth=16):
+    """The engine's cell capacity: n leaves plus, per depth d < 16, at most
+    min(4^d, n // (bucket + 1)) internal cells."""
+    return n + sum(min(4 ** d, n // (bucket + 1)) for d in range(depth)) + 1
+
+
+@pytest.mark.parametrize("layout,bucket", [("grid", 1), ("random", 1), ("random", 4)])
+def test_worst_case_cell_counts_fit_the_capacity(gpu, rt, oracle, layout, bucket):
+    # groups of bucket+1 coincident bodies, each group alone in its cell from
+    # a shallow depth on: every group is a chain of internal cells down to
+    # depth 16, the tree that comes closest to the arena's cell capacity
+    rng = np.random.default_rng(9)
+    groups = 1 << 15 if bucket == 1 else 1 << 13
+    if layout == "grid":
+        side = int(np.sqrt(groups))
+        xs = (np.arange(side) + 0.5) / side
+        gx, gy = np.meshgrid(xs, xs)
+        centers = np.stack([gx.ravel(), gy.ravel()], axis=1)
+    else:
+        centers = rng.random((groups, 2))
+    pts = np.repeat(centers, bucket + 1, axis=0)
+    bodies = np.zeros((len(pts), 5))
+    bodies[:, :2] = pts
+    bodies[:, 4] = 1.0 / len(pts)
+    cfg = Config(bucket=bucket, g=1.0, softening_kpc=0.01)
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    assert_tree_bit_exact(oracle, evid, ot, b32, oc, cfg)
+    assert len(ot.cells) > 0.65 * _cell_bound(len(pts), bucket)
+
+
 @pytest.mark.parametrize("theta", [0.0, 0.3, 0.5, 0.7, 2.0])
 def test_forces_match_reference_traversal(gpu, rt, oracle, theta):
     cfg = Config(theta=theta, softening_kpc=0.01, g=1.0, bucket=1)
