@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -685,8 +686,14 @@ extern "C" int galaxy_bh_batch_footprint(const uint32_t* counts, const bh_config
     return BH_OK;
 }
 
+// Builds a batch of `count` states.  A `donor` batch of the same device
+// handle (or null) gives up its arena when that is large enough, and is
+// freed either way: re-forming a batch, or pointing a tree at another state,
+// then allocates nothing (the donor's work precedes the new batch's on the
+// handle's stream).
 static int batch_build(bh_device* dev, bh_state* const* states, const bh_config* cfgs,
-                       uint32_t count, Batch** out) {
+                       uint32_t count, Batch** out, Batch* donor_batch = nullptr) {
+    std::unique_ptr<Batch> donor(donor_batch);
     *out = nullptr;
     if (!count) return set_error(BH_INVALID_ARG, "batch needs at least one state");
     std::vector<uint32_t> counts(count);
@@ -712,17 +719,25 @@ static int batch_build(bh_device* dev, bh_state* const* states, const bh_config*
     b->cell_capacity = L.cells;
     b->arena_bytes = A.total();
     cudaError_t e = cudaSuccess;
+    if (donor && donor->arena && donor->arena_capacity >= b->arena_bytes) {
+        b->arena = donor->arena;
+        b->arena_capacity = donor->arena_capacity;
+        donor->arena = nullptr;
+    }
+    donor.reset();  // a donor arena too small goes back to the pool first
     // the arena comes from the device handle's stream-ordered pool, which
     // keeps released arenas and state buffers for reuse
-    e = cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, dev->pool, dev->stream);
-    if (e == cudaErrorMemoryAllocation) {
-        // give back what the pool keeps, then retry
-        cudaGetLastError();
-        cudaStreamSynchronize(dev->stream);
-        cudaMemPoolTrimTo(dev->pool, 0);
+    if (!b->arena) {
         e = cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, dev->pool, dev->stream);
+        if (e == cudaErrorMemoryAllocation) {
+            // give back what the pool keeps, then retry
+            cudaGetLastError();
+            cudaStreamSynchronize(dev->stream);
+            cudaMemPoolTrimTo(dev->pool, 0);
+            e = cudaMallocFromPoolAsync(&b->arena, b->arena_bytes, dev->pool, dev->stream);
+        }
+        b->arena_capacity = b->arena_bytes;
     }
-    b->arena_capacity = b->arena_bytes;
     if (e != cudaSuccess) {
         b->arena = nullptr;
         delete b;
@@ -978,6 +993,33 @@ extern "C" int galaxy_bh_tree_destroy(bh_tree* tree) {
     bh_device* dev = tree->dev;
     delete tree;
     device_unref(dev);
+    return BH_OK;
+}
+
+// Points *tree at state st under cfg (creating the tree when null), keeping
+// its arena when that is large enough: a serving loop's stager solves each
+// newcomer's boundary on one tree instead of allocating one per request.
+int gbh::tree_retarget(bh_device* dev, bh_tree** tree, bh_state* st, const bh_config* cfg) {
+    if (!tree) return set_error(BH_INVALID_ARG, "null argument");
+    if (!*tree) return galaxy_bh_tree_create(dev, st, cfg, tree);
+    int rc = enter(dev);
+    if (rc) return rc;
+    bh_tree* t = *tree;
+    if (!st) return set_error(BH_INVALID_ARG, "null argument");
+    if (t->dev != dev || st->dev != dev)
+        return set_error(BH_INVALID_ARG, "tree or state belongs to another device handle");
+    if ((rc = validate_config(cfg))) return rc;
+    Batch* b = nullptr;
+    Batch* donor = t->batch;
+    t->batch = nullptr;
+    t->built = false;
+    if ((rc = batch_build(dev, &st, cfg, 1, &b, donor))) {
+        galaxy_bh_tree_destroy(t);
+        *tree = nullptr;
+        return rc;
+    }
+    t->batch = b;
+    t->st = st;
     return BH_OK;
 }
 
@@ -1358,6 +1400,42 @@ extern "C" int galaxy_bh_batch_destroy(bh_batch* batch) {
     bh_device* dev = batch->dev;
     delete batch;
     device_unref(dev);
+    return BH_OK;
+}
+
+// Re-forms *batch over `count` states (creating it when null, destroying it
+// when count is 0), keeping its arena when that is large enough: a serving
+// loop's joins and leaves then allocate nothing once the arena has grown to
+// the largest active set.
+int gbh::batch_reform(bh_device* dev, bh_batch** batch, bh_state* const* states,
+                      const bh_config* cfgs, uint32_t count) {
+    if (!batch) return set_error(BH_INVALID_ARG, "null argument");
+    if (count == 0) {
+        galaxy_bh_batch_destroy(*batch);
+        *batch = nullptr;
+        return BH_OK;
+    }
+    if (!*batch) return galaxy_bh_batch_create(dev, states, cfgs, count, batch);
+    int rc = enter(dev);
+    if (rc) return rc;
+    bh_batch* h = *batch;
+    if (h->dev != dev) return set_error(BH_INVALID_ARG, "batch belongs to another device handle");
+    if (!states || !cfgs) return set_error(BH_INVALID_ARG, "null argument");
+    for (uint32_t s = 0; s < count; ++s)
+        if (cfgs[s].flags & BH_FLAG_POTENTIAL) {
+            if (!states[s]) return set_error(BH_INVALID_ARG, "null state %u", s);
+            if ((rc = ensure_potential(states[s]))) return rc;
+        }
+    Batch* b = nullptr;
+    Batch* donor = h->batch;
+    h->batch = nullptr;
+    h->solved = false;
+    if ((rc = batch_build(dev, states, cfgs, count, &b, donor))) {
+        galaxy_bh_batch_destroy(h);
+        *batch = nullptr;
+        return rc;
+    }
+    h->batch = b;
     return BH_OK;
 }
 

@@ -167,6 +167,13 @@ cudaError_t launch_check_records(const void* records, int kind, uint32_t n, uint
 // `to`, after the state's pending work (bh_engine.cu).
 int state_move(bh_state* st, bh_device* to);
 
+// Re-forms *batch over new members, or points *tree at another state,
+// reusing the arena when it is large enough (bh_engine.cu); null creates,
+// a failure leaves null.
+int batch_reform(bh_device* dev, bh_batch** batch, bh_state* const* states,
+                 const bh_config* cfgs, uint32_t count);
+int tree_retarget(bh_device* dev, bh_tree** tree, bh_state* st, const bh_config* cfg);
+
 // Sets the calling thread's last-error message (bh_engine.cu); returns status.
 int set_error_message(int status, const char* message);
 

@@ -81,19 +81,16 @@ void release_state(std::unique_ptr<ServeRequest>& r) {
     r->st = nullptr;
 }
 
-// Replaces *b by a batch of the active requests from index `from` on.
-int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active, bh_batch** b,
-               size_t from = 0) {
-    if (*b) galaxy_bh_batch_destroy(*b);
-    *b = nullptr;
-    if (active.size() <= from) return BH_OK;
+// Re-forms *b over the active requests, reusing its arena when it is large
+// enough (the arena grows to the largest active set and stays).
+int form_batch(bh_server* s, std::vector<std::unique_ptr<ServeRequest>>& active, bh_batch** b) {
     std::vector<bh_state*> states;
     std::vector<bh_config> cfgs;
-    for (size_t i = from; i < active.size(); ++i) {
-        states.push_back(active[i]->st);
-        cfgs.push_back(active[i]->cfg);
+    for (auto& r : active) {
+        states.push_back(r->st);
+        cfgs.push_back(r->cfg);
     }
-    return galaxy_bh_batch_create(s->dev, states.data(), cfgs.data(), (uint32_t)states.size(), b);
+    return gbh::batch_reform(s->dev, b, states.data(), cfgs.data(), (uint32_t)states.size());
 }
 
 // Whether `cand` joins the active members and the staged requests inside
@@ -134,6 +131,9 @@ void stage_loop(bh_server* s) {
     // serving loop's own small uploads behind this one
     GpuEvolveState* pinned = nullptr;
     size_t pinned_n = 0;
+    // one tree, pointed at each newcomer in turn: its arena grows to the
+    // largest request solved and is then reused
+    bh_tree* tree = nullptr;
     while (true) {
         std::unique_ptr<ServeRequest> r;
         int rc = BH_OK;
@@ -171,13 +171,11 @@ void stage_loop(bh_server* s) {
         }
         const double t1 = s->now();
         if (rc == BH_OK) {
-            bh_tree* tree = nullptr;
-            rc = galaxy_bh_tree_create(s->dev2, r->st, &r->cfg, &tree);
+            rc = gbh::tree_retarget(s->dev2, &tree, r->st, &r->cfg);
             if (rc == BH_OK) rc = galaxy_bh_tree_rebuild(s->dev2, r->st, tree, &r->cfg, nullptr);
             bh_config fc = r->cfg;
             fc.flags |= BH_FLAG_NO_STATS;
             if (rc == BH_OK) rc = galaxy_bh_force(s->dev2, r->st, tree, &fc, nullptr);
-            if (tree) galaxy_bh_tree_destroy(tree);
             if (rc == BH_OK) rc = gbh::state_move(r->st, s->dev);
         }
         const double t2 = s->now();
@@ -197,6 +195,7 @@ void stage_loop(bh_server* s) {
         s->staged.push_back(std::move(r));
         s->cv_in.notify_all();
     }
+    if (tree) galaxy_bh_tree_destroy(tree);
     if (pinned) cudaFreeHost(pinned);
 }
 
