@@ -1470,6 +1470,9 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
         if (POT) phi -= take ? gm * inv_r : 0.f;
     };
     const uint32_t lane_bit = 1u << lane;
+    // A lane outside an entry's mask may sit at distance 0 from it (its own
+    // body, with zero softening): its scale is selected to 0 after the
+    // product, so the inf of that product never reaches the sums.
     auto flush = [&](uint32_t count) {
 #pragma unroll 4
         for (uint32_t i = 0; i < count; ++i) {
@@ -1478,15 +1481,13 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
             if constexpr (COMP) d = __fadd2_rn(d, s_lo[warp][i]);
             const float inv_r = rsqrtf(__fmaf_rn(d.x, d.x, __fmaf_rn(d.y, d.y, eps2)));
             const bool take = (__float_as_uint(e.w) & lane_bit) != 0u;
+            const float scale = e.z * inv_r * inv_r * inv_r;
             if constexpr (!COMP && !POT) {
                 // plain sums: lanes outside the mask skip the (predicated) adds
-                const float scale = e.z * inv_r * inv_r * inv_r;
                 if (take) acc.add_scaled(d, scale);
             } else {
-                const float gm = take ? e.z : 0.f;
-                const float scale = gm * inv_r * inv_r * inv_r;
-                acc.add_scaled(d, scale);
-                if (POT) phi -= gm * inv_r;
+                acc.add_scaled(d, take ? scale : 0.f);
+                if (POT) phi -= take ? e.z * inv_r : 0.f;
             }
         }
     };

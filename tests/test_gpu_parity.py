@@ -565,6 +565,27 @@ def test_forces_on_small_and_degenerate_systems(gpu, rt, oracle, case):
     assert np.isfinite(gpu.read_evolving_state(ev)[0]).all()
 
 
+@pytest.mark.parametrize("form", ["plain", "compensated", "potential"])
+def test_zero_softening_forces_finite_and_within_tolerance(gpu, rt, oracle, form):
+    """Softening 0 (admitted by the config checks): a lane whose own body is
+    an interaction-list entry that the other lanes take sits at distance 0
+    from it; its forces stay finite and within tolerance in every summation
+    form, and the potential form reproduces the plain accelerations."""
+    bodies = scenarios.exponential_disc(4096, 17)
+    cfg = Config(theta=0.5, softening_kpc=0.0, g=1.0, bucket=1,
+                 compensated=form == "compensated", potential=form == "potential")
+    ev, tree, evid, ot, b32, oc = build_both(gpu, rt, oracle, bodies, cfg)
+    rt.force(gpu, ev, tree, cfg)
+    acc, _ = gpu.read_evolving_accelerations(ev)
+    assert np.isfinite(acc).all()
+    force_check(oracle, acc, b32, ot, oc)
+    if form == "potential":
+        plain = Config(theta=0.5, softening_kpc=0.0, g=1.0, bucket=1)
+        rt.force(gpu, ev, tree, plain)
+        acc_plain, _ = gpu.read_evolving_accelerations(ev)
+        assert np.array_equal(acc, acc_plain)
+
+
 @pytest.mark.slow
 def test_large_n_tree_and_sampled_forces(gpu, rt, oracle):
     """N = 2^23: the whole tree bit-exact (Morton codes, permutation and the
