@@ -323,10 +323,11 @@ int galaxy_bh_batch_bytes(bh_batch* batch, uint64_t* bytes);
  * advance together in rounds of at most round_steps fused KDK steps in one
  * batch; a round stops at the smallest remaining step count so finished
  * simulations leave and waiting ones join between rounds.  Each result
- * equals the same simulation stepped alone.  Outside the budget the server
- * keeps, once grown, the batch arena of its largest active set and the
- * stager's tree arena of its largest request (reused, not reallocated, at
- * every join and leave) in the handles' memory pools.  submit copies the initial
+ * equals the same simulation stepped alone.  The budget counts the current
+ * members; beyond it the server keeps, once grown, the batch arena of its
+ * largest active set so far and the stager's tree arena of its largest
+ * request (reused at every join and leave instead of reallocated).  submit
+ * copies the initial
  * records; poll waits up to timeout_ms for a finished request (BH_TIMEOUT if
  * none), fills *result (status = the request's bh_status: a request that can
  * never fit the budget fails with BH_CAPACITY_OVERFLOW) and copies its final
