@@ -393,13 +393,20 @@ def per_body_force_error(gpu, rt, ev, tree, cfg) -> dict:
     traversal of the same tree (galaxy_bh_force_f64, flat.rs:270-371, the
     same cells, order and f64 arithmetic as the CPU reference), at every
     body; for the bodies above 1e-5, S/|a| (S = sum of the body's term
-    magnitudes) says how far their terms cancel.  Leaves the plain forces
-    (the step's own) in the state."""
-    ref, s, _ = rt.force_f64(gpu, ev, tree, cfg, abs_sum=True)
+    magnitudes) says how far their terms cancel.  The opening decisions
+    are compared through the two traversals' counters (cells visited,
+    approximated, bodies summed directly): their differences count MAC flips
+    in aggregate.  Leaves the plain forces (the step's own) in the state."""
+    ref, s, f64_counts = rt.force_f64(gpu, ev, tree, cfg, abs_sum=True)
     mag = np.hypot(ref[:, 0], ref[:, 1])
     ratio = s / np.maximum(mag, 1e-300)
     out = {"against": "galaxy_bh_force_f64 (reference f64 flat traversal, same tree)",
            "bodies": int(len(ref)), "S_over_a_median": r4(float(np.median(ratio)))}
+    rt.force(gpu, ev, tree, dataclasses.replace(cfg, compensated=False, force_stats=True))
+    f32_counts = rt.force_stats(gpu, tree)
+    out["decisions"] = {"f64": f64_counts, "f32": {k: f32_counts[k] for k in f64_counts},
+                        "differences": {k: int(f32_counts[k] - v) for k, v in f64_counts.items()},
+                        "identical": all(f32_counts[k] == v for k, v in f64_counts.items())}
     for name, comp in (("compensated", True), ("plain", False)):
         c = dataclasses.replace(cfg, compensated=comp, force_stats=False)
         rt.force(gpu, ev, tree, c)
@@ -675,6 +682,7 @@ def run_engine(args, world, rank, local, pg):
                                     "fraction": per_body[k]["fraction_above"],
                                     "max": per_body[k]["max"]}
                                 for k in ("plain", "compensated")},
+        "mac_decision_counts_identical": per_body["decisions"]["identical"],
         "same_tree_kernels_ms": {k: v for k, v in kernels.items() if k.endswith("_ms")},
         "e2e": r4(e2e_value),
     }
