@@ -1,16 +1,19 @@
 // SPDX-License-Identifier: Apache-2.0
 // Native continuous-batching server over the public C ABI (galaxy_bh.h).
 //
-// One host thread owns a device handle and runs the serving loop: submitted
-// requests (initial state records, config, dt, step count) wait in arrival
-// order and are admitted as soon as the device-memory footprint of the
-// active set plus the newcomer fits the budget; admitted simulations stay
-// resident and advance together, a round of fused KDK steps at a time, in one
-// batch (one launch per stage for all of them).  A round stops at the
-// smallest remaining step count, so finished simulations leave and waiting
-// ones join between rounds.  Finished results are copied back and queued for
-// galaxy_bh_serve_poll.  Each simulation's result equals its result alone:
-// batch members never interact.
+// Two host threads, each owning a device handle (and so a stream) of the
+// same GPU.  The stager takes submitted requests (initial state records,
+// config, dt, step count) in arrival order as soon as the device-memory
+// footprint of the active set, the staged requests and the newcomer fits
+// the budget; it uploads and checks the newcomer's state and solves its
+// boundary acceleration while the rounds go on, then hands the state to the
+// serving loop's handle.  The serving loop admits staged requests between
+// rounds; admitted simulations stay resident and advance together, a round
+// of fused KDK steps at a time, in one batch (one launch per stage for all
+// of them).  A round stops at the smallest remaining step count, so finished
+// simulations leave and staged ones join between rounds.  Finished results
+// are copied back and queued for galaxy_bh_serve_poll.  Each simulation's
+// result equals its result alone: batch members never interact.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -120,8 +123,9 @@ constexpr size_t kStageAhead = 4;  // requests the stager prepares ahead of admi
 
 // The stager: in arrival order, for the requests that fit the budget next to
 // the active and the already staged ones, uploads and checks the initial
-// state and runs its boundary solve (rebuild + force, a tree of its own) on
-// the stager's handle and stream, so that this host work and its copies
+// state and runs its boundary solve (rebuild + force on the stager's own
+// tree, reused from request to request) on the stager's handle and stream,
+// so that this host work and its copies
 // overlap the rounds the loop keeps running; then hands the state to the
 // loop's handle.  A simulation's result does not depend on where its solve
 // ran: the tree kernels are the same.
