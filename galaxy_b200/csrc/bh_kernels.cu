@@ -800,7 +800,10 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
 // window) never touch global memory.
 // Positions per k_aggregate block: cells whose range crosses a multiple of it
 // are finished by cross-block climbs (the only users of the cell counters).
-constexpr uint32_t kAggBlockPositions = 256;
+#ifndef GBH_AGG_POSITIONS
+#define GBH_AGG_POSITIONS 256
+#endif
+constexpr uint32_t kAggBlockPositions = GBH_AGG_POSITIONS;
 constexpr uint32_t kCellsThreads = 256;
 constexpr uint32_t kCellsWin = 1024;
 constexpr uint32_t kMaxChain = kMortonDepth + 1;  // cells per position: depths 0..16
@@ -1224,15 +1227,19 @@ __device__ void climb(const AggArgs& a, uint32_t k) {
 // 64 threads per 256 positions: a depth holds few cells, and small blocks
 // let many blocks hide each other's per-depth latency.
 constexpr uint32_t kAggPositions = kAggBlockPositions;
-constexpr uint32_t kAggThreads = 64;
+#ifndef GBH_AGG_THREADS
+#define GBH_AGG_THREADS 64
+#endif
+constexpr uint32_t kAggThreads = GBH_AGG_THREADS;
 
 __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint32_t npos,
                                                            const uint32_t* __restrict__ base,
                                                            uint32_t* err) {
     wait_for_predecessor();
-    // local internal cells by depth (offsets from kb): one cell per position
-    // and depth, internal depths 0..15
-    __shared__ uint16_t s_level[kMortonDepth][kAggPositions];
+    // local internal cells by depth (offsets from kb), internal depths
+    // 0..15: those of one depth hold disjoint ranges of at least two
+    // positions, so at most half the block's positions per depth
+    __shared__ uint16_t s_level[kMortonDepth][kAggPositions / 2];
     __shared__ uint32_t s_count[kMortonDepth];
     __shared__ uint32_t s_code[kAggPositions + 2];  // codes of positions P0-1 .. P0+256
     const uint32_t t = threadIdx.x;
@@ -1264,17 +1271,16 @@ __global__ void __launch_bounds__(kAggThreads) k_aggregate(const AggArgs a, uint
             aggregate_cell(a, k, u, true);
             if (u.w > 0 && !inside(u.z, u.w - 1u, sd)) climb(a, k);
         } else if (inside(u.z, u.w, sd)) {
-            if (u.w < kMortonDepth) {
-                const uint32_t slot = atomicAdd(&s_count[u.w], 1u);
+            const uint32_t slot = u.w < kMortonDepth ? atomicAdd(&s_count[u.w], 1u) : kNone;
+            if (slot < kAggPositions / 2)
                 s_level[u.w][slot] = (uint16_t)(k - kb);
-            } else {
+            else
                 set_err(err, kErrCapacity);
-            }
         }
     }
     __syncthreads();
     for (int d = (int)kMortonDepth - 1; d >= 0; --d) {
-        const uint32_t cnt = s_count[d];
+        const uint32_t cnt = min(s_count[d], kAggPositions / 2);
         if (cnt == 0) continue;
         for (uint32_t j = t; j < cnt; j += kAggThreads) {
             const uint32_t k = kb + s_level[d][j];
