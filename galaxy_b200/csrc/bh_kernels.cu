@@ -493,7 +493,10 @@ __global__ void __launch_bounds__(kMortonThreads) k_morton(const SimDesc* __rest
 
 // ============================================================== radix =====
 
-constexpr int kLookWindow = 8;  // predecessor flags loaded per look-back round trip
+#ifndef GBH_LOOK_WINDOW
+#define GBH_LOOK_WINDOW 8
+#endif
+constexpr int kLookWindow = GBH_LOOK_WINDOW;  // predecessor flags loaded per look-back round trip
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = (1u << 30) - 1u;
