@@ -1284,14 +1284,14 @@ static int run_packed(bh_device* dev, const BhSettings* settings, const GpuBody*
         (e = cudaMalloc(&d_b, sizeof(GpuBody) * (size_t)n)) ||
         (e = cudaMalloc(&d_e, sizeof(GpuEntry) * (size_t)n)) ||
         (e = cudaMalloc(&d_c, sizeof(GpuCell) * (size_t)cell_count)) ||
-        (e = cudaMalloc(&d_err, 4)))
+        (e = cudaMalloc(&d_err, 8)))
         goto done;
     cudaEventRecord(dev->ev[0], s);
     if ((e = cudaMemcpyAsync(d_s, settings, sizeof(BhSettings), cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(d_b, bodies, sizeof(GpuBody) * (size_t)n, cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(d_e, entries, sizeof(GpuEntry) * (size_t)n, cudaMemcpyHostToDevice, s)) ||
         (e = cudaMemcpyAsync(d_c, cells, sizeof(GpuCell) * (size_t)cell_count, cudaMemcpyHostToDevice, s)) ||
-        (e = cudaMemsetAsync(d_err, 0, 4, s)))
+        (e = cudaMemsetAsync(d_err, 0, 8, s)))
         goto done;
     cudaEventRecord(dev->ev[1], s);
     if ((e = launch_traverse_packed(d_s, d_b, d_e, d_c, n, cell_count, d_out, d_err, s))) goto done;

@@ -137,6 +137,8 @@ cudaError_t launch_traverse(const BatchBuffers& b, bool compensated, bool plain,
                             bool stats, cudaStream_t s);
 cudaError_t launch_export(const BatchBuffers& b, uint32_t sim, GpuEntry* entries, GpuBody* bodies,
                           GpuCell* cells, cudaStream_t s);
+// err: two zeroed words, the error bits and a flag the launch sets when the
+// packed entries and bodies disagree.
 cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bodies,
                                    const GpuEntry* entries, const GpuCell* cells, uint32_t n,
                                    uint32_t ncells, float4* accel, uint32_t* err,

@@ -1670,8 +1670,8 @@ __global__ void __launch_bounds__(WARPS * 32, GBH_TRAVERSE_MIN_BLOCKS * kTravWar
 
 // runtime/src/nbody.wgsl:43-123 (and barnes_hut_flat.cu:65-146) over an
 // arbitrary packed tree with explicit children: the same per-body decisions
-// (f32 MAC with sqrt) and order, computed warp-cooperatively over 32
-// consecutive Morton positions with a shared (cell, lane mask) stack.
+// (f32 MAC with sqrt), self-exclusion and terms, computed for a warp of 32
+// consecutive Morton positions at once.
 constexpr int kPackedStack = 64;
 
 __device__ __forceinline__ void packed_point_mass(float tx, float ty, float px, float py,
@@ -1686,35 +1686,45 @@ __device__ __forceinline__ void packed_point_mass(float tx, float ty, float px, 
     *ay += dy * scale;
 }
 
-__global__ void __launch_bounds__(256) k_traverse_packed(
-    const BhSettings* __restrict__ settings, const GpuBody* __restrict__ bodies,
-    const GpuEntry* __restrict__ entries, const GpuCell* __restrict__ cells, uint32_t n,
-    uint32_t ncells, float4* __restrict__ accel, uint32_t* err) {
-    __shared__ uint32_t s_cell[8][kPackedStack];
-    __shared__ uint32_t s_mask[8][kPackedStack];
-    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-    const uint32_t p = (blockIdx.x * 8 + warp) * 32u + lane;
-    if ((blockIdx.x * 8 + warp) * 32u >= n) return;
-    const BhSettings st = *settings;
+// Whether every position's entry names a body whose recorded Morton
+// position is that position (bodies[entries[p].body].meta[0] == p), i.e. the
+// entries are a permutation of the bodies and meta its inverse, as
+// pack_flat_tree writes them.  *bad gets 1 otherwise.  The lane-parallel
+// walk relies on it: a lane's own body is the one at its position.
+__global__ void k_check_packed(const GpuBody* __restrict__ bodies,
+                               const GpuEntry* __restrict__ entries, uint32_t n, uint32_t* bad) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t o = entries[p].data[1];
+    if (o >= n || bodies[o].meta[0] != p) atomicOr(bad, 1u);
+}
+
+// The walk one cell at a time: every lane of the warp tests the same cell
+// and keeps the reference's depth-first order of its own terms (children
+// pushed 3..0).  Used when the entries and bodies disagree or a tree is
+// deeper than the lane-parallel walk's stack bound.  s_cell / s_mask hold
+// kPackedStack entries each.
+__device__ void packed_walk_cellwise(const BhSettings& st, const GpuBody* __restrict__ bodies,
+                                     const GpuEntry* __restrict__ entries,
+                                     const GpuCell* __restrict__ cells, uint32_t n,
+                                     uint32_t ncells, uint32_t ti, float tx, float ty,
+                                     uint32_t tpos, bool lane_ok, uint32_t* s_cell,
+                                     uint32_t* s_mask, uint32_t* err, float* out_ax,
+                                     float* out_ay) {
     const float theta = st.physics[0], soft = st.physics[1], g = st.physics[2];
-    const bool valid = p < n;
-    const uint32_t ti = valid ? entries[p].data[1] : 0u;
-    const bool ti_ok = ti < n;
-    const GpuBody tb = (valid && ti_ok) ? bodies[ti] : GpuBody{};
-    const float tx = tb.position_mass[0], ty = tb.position_mass[1];
-    const uint32_t tpos = tb.meta[0];
+    const uint32_t lane = lane_id();
     float ax = 0.f, ay = 0.f;
     int len = 1;
-    const uint32_t vmask = __ballot_sync(kFull, valid && ti_ok);
+    const uint32_t vmask = __ballot_sync(kFull, lane_ok);
     if (lane == 0) {
-        s_cell[warp][0] = st.info[2];
-        s_mask[warp][0] = vmask;
+        s_cell[0] = st.info[2];
+        s_mask[0] = vmask;
     }
     __syncwarp();
     while (len > 0) {
         --len;
-        const uint32_t ci = s_cell[warp][len];
-        const uint32_t M = s_mask[warp][len];
+        const uint32_t ci = s_cell[len];
+        const uint32_t M = s_mask[len];
         __syncwarp();
         if (ci >= ncells) {
             set_err(err, kErrPackedIndex);
@@ -1769,8 +1779,8 @@ __global__ void __launch_bounds__(256) k_traverse_packed(
             if (lane == 0) {
                 for (int q = 3; q >= 0; --q) {
                     if (cell.children[q] != GALAXY_BH_NO_CHILD) {
-                        s_cell[warp][len] = cell.children[q];
-                        s_mask[warp][len] = O;
+                        s_cell[len] = cell.children[q];
+                        s_mask[len] = O;
                         ++len;
                     }
                 }
@@ -1779,7 +1789,233 @@ __global__ void __launch_bounds__(256) k_traverse_packed(
             __syncwarp();
         }
     }
-    if (valid && ti_ok) accel[ti] = make_float4(ax, ay, 0.f, 0.f);
+    *out_ax = ax;
+    *out_ay = ay;
+}
+
+// Lane-parallel walk over the packed tree, the structure of k_traverse: a
+// warp pops up to 8 opened cells from its shared-memory stack and lane 4i+q
+// examines child q of popped cell i for all lanes of its mask at once,
+// against the bounding box of the warp's bodies.  The reference decides in
+// f32: a lane approximates a cell unless the cell holds its own body, if
+// its squared distance d2 to the centre of mass is positive and
+// (2 half) / sqrt(d2) < theta.  d2 = fma(dx, dx, dy*dy), sqrt and the
+// division are monotone in |dx|, |dy| (round to nearest), so the test at
+// the box's nearest point (all lanes approximate) or farthest corner (all
+// open) is every lane's own test; other cells are decided lane by lane
+// with the same expression.  Approximated cells and one-body leaves go to
+// the interaction list, several-body leaves are summed body by body; a
+// lane's own body is the one at its position (the entries are checked to be
+// a permutation whose inverse the bodies record), so self-exclusion is
+// the lane bit of that position.  Each lane sums exactly the reference's
+// terms; only their order differs.
+constexpr uint32_t kPkWarps = 4;
+constexpr uint32_t kPkRoot = 0xfffffffeu;  // stack entry standing for the root cell itself
+// (cell, lane mask) entries: the stack stays sorted by depth and one step
+// pushes at most 32 opened cells, so 32 per level of a tree of depth 16
+// (pack_flat_tree's trees); a deeper tree that overflows it is walked again
+// cell by cell
+constexpr uint32_t kPkStack = 17u * 32u;
+static_assert(2u * kPkStack >= 2u * kPackedStack, "the cell-by-cell walk borrows the stack");
+
+__global__ void __launch_bounds__(kPkWarps * 32) k_traverse_packed(
+    const BhSettings* __restrict__ settings, const GpuBody* __restrict__ bodies,
+    const GpuEntry* __restrict__ entries, const GpuCell* __restrict__ cells, uint32_t n,
+    uint32_t ncells, float4* __restrict__ accel, uint32_t* err,
+    const uint32_t* __restrict__ inconsistent) {
+    __shared__ uint2 s_stack[kPkWarps][kPkStack];
+    __shared__ float4 s_list[kPkWarps][kTravList];  // (x, y, G*m, lane mask bits)
+    __shared__ uint32_t s_mix[kPkWarps][32][2];      // mixed cells by rank: deciding, opened
+    const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint32_t p0 = (blockIdx.x * kPkWarps + warp) * 32u;
+    if (p0 >= n) return;
+    const BhSettings st = *settings;
+    const float theta = st.physics[0], soft = st.physics[1], g = st.physics[2];
+    const uint32_t p = p0 + lane;
+    const bool valid = p < n;
+    const uint32_t ti = valid ? entries[p].data[1] : 0u;
+    const bool ti_ok = ti < n;
+    const GpuBody tb = (valid && ti_ok) ? bodies[ti] : GpuBody{};
+    const float tx = tb.position_mass[0], ty = tb.position_mass[1];
+    uint32_t* s_cell = reinterpret_cast<uint32_t*>(s_stack[warp]);
+    float ax = 0.f, ay = 0.f;
+    if (*inconsistent) {
+        packed_walk_cellwise(st, bodies, entries, cells, n, ncells, ti, tx, ty, tb.meta[0],
+                             valid && ti_ok, s_cell, s_cell + kPackedStack, err, &ax, &ay);
+        if (valid && ti_ok) accel[ti] = make_float4(ax, ay, 0.f, 0.f);
+        return;
+    }
+    // consistent input: every valid lane's body is ti, at position p
+    const float eps2 = soft * soft;
+    const uint32_t valid_mask = __ballot_sync(kFull, valid);
+    const uint32_t lanes_below = (1u << lane) - 1u;
+    const uint32_t lane_bit = 1u << lane;
+    float bx0 = valid ? tx : INFINITY, bx1 = valid ? tx : -INFINITY;
+    float by0 = valid ? ty : INFINITY, by1 = valid ? ty : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        bx0 = fminf(bx0, __shfl_xor_sync(kFull, bx0, o));
+        bx1 = fmaxf(bx1, __shfl_xor_sync(kFull, bx1, o));
+        by0 = fminf(by0, __shfl_xor_sync(kFull, by0, o));
+        by1 = fmaxf(by1, __shfl_xor_sync(kFull, by1, o));
+    }
+    uint2* stack = s_stack[warp];
+    float4* list = s_list[warp];
+    // one point-mass term (the reference's add_point_mass) for lanes that take it
+    auto term = [&](float dx, float dy, float gm, bool take) {
+        const float inv_r = rsqrtf(__fmaf_rn(dx, dx, __fmaf_rn(dy, dy, eps2)));
+        const float scale = gm * inv_r * inv_r * inv_r;
+        if (take) {
+            ax += dx * scale;
+            ay += dy * scale;
+        }
+    };
+    auto flush = [&](uint32_t count) {
+#pragma unroll 4
+        for (uint32_t i = 0; i < count; ++i) {
+            const float4 e = list[i];
+            term(e.x - tx, e.y - ty, e.z, (__float_as_uint(e.w) & lane_bit) != 0u);
+        }
+    };
+    // the reference's opening test: true = approximate
+    auto approximates = [&](float two_half, float d2) {
+        return d2 > 0.0f && two_half / sqrtf(d2) < theta;
+    };
+
+    if (lane == 0) stack[0] = make_uint2(kPkRoot, valid_mask);
+    __syncwarp();
+    uint32_t len = 1, nlist = 0;
+    bool overflow = false;
+    while (len > 0) {
+        const uint32_t ng = min(len, 8u);
+        const uint32_t gi = lane >> 2, q = lane & 3u;
+        const bool have = gi < ng;
+        uint2 e = make_uint2(0u, 0u);
+        if (have) e = stack[len - ng + gi];
+        __syncwarp();
+        len -= ng;
+        uint32_t c = GALAXY_BH_NO_CHILD;
+        if (have) c = e.x == kPkRoot ? (q == 0u ? st.info[2] : GALAXY_BH_NO_CHILD)
+                                     : __ldg(&cells[e.x].children[q]);
+        bool present = c != GALAXY_BH_NO_CHILD;
+        if (present && c >= ncells) {
+            set_err(err, kErrPackedIndex);
+            present = false;
+        }
+        float4 chm = make_float4(0.f, 0.f, 0.f, 0.f);  // centre, half, mass
+        float2 com = make_float2(0.f, 0.f);
+        uint4 rd = make_uint4(0u, 0u, 0u, 0u);          // start, end, depth, valid
+        uint4 chn = make_uint4(GALAXY_BH_NO_CHILD, GALAXY_BH_NO_CHILD, GALAXY_BH_NO_CHILD,
+                               GALAXY_BH_NO_CHILD);
+        if (present) {
+            const GpuCell* cr = cells + c;
+            chm = __ldg(reinterpret_cast<const float4*>(cr->center_half_mass));
+            com = __ldg(reinterpret_cast<const float2*>(cr->com));
+            rd = __ldg(reinterpret_cast<const uint4*>(cr->range_depth));
+            chn = __ldg(reinterpret_cast<const uint4*>(cr->children));
+        }
+        const uint32_t A = e.y;
+        const bool leaf = chn.x == GALAXY_BH_NO_CHILD && chn.y == GALAXY_BH_NO_CHILD &&
+                          chn.z == GALAXY_BH_NO_CHILD && chn.w == GALAXY_BH_NO_CHILD;
+        // lanes whose own body the cell holds: positions [start, end)
+        const uint32_t ha = max(rd.x, p0), hb = min(rd.y, p0 + 32u);
+        const uint32_t H = (present && ha < hb) ? bit_range(ha - p0, hb - p0) : 0u;
+        const uint32_t R = A & ~H;
+        const bool internal = present && !leaf;
+        const bool one = present && leaf && rd.y == rd.x + 1u;
+        const bool multi = present && leaf && rd.y > rd.x + 1u;
+        // a one-body leaf is a term at its body (the reference sums leaves
+        // from the bodies themselves)
+        float ex = com.x, ey = com.y, em = chm.w;
+        if (one) {
+            if (rd.x < n) {
+                const float4 b = __ldg(reinterpret_cast<const float4*>(
+                    bodies[__ldg(&entries[rd.x].data[1])].position_mass));
+                ex = b.x;
+                ey = b.y;
+                em = b.z;
+            } else {
+                set_err(err, kErrPackedIndex);
+            }
+        }
+        const float two_half = 2.0f * chm.z;
+        const float nx = fmaxf(fmaxf(bx0 - com.x, com.x - bx1), 0.f);
+        const float ny = fmaxf(fmaxf(by0 - com.y, com.y - by1), 0.f);
+        const float fx = fmaxf(fabsf(com.x - bx0), fabsf(com.x - bx1));
+        const float fy = fmaxf(fabsf(com.y - by0), fabsf(com.y - by1));
+        const bool far = internal && approximates(two_half, dist2(nx, ny));
+        const bool near = internal && !approximates(two_half, dist2(fx, fy));
+        const uint32_t ap = (one || far) ? R : 0u;
+        uint32_t op = internal ? ((A & H) | (near ? R : 0u)) : 0u;
+        const bool mixed = internal && R != 0u && !far && !near;
+
+        // mixed cells: every lane of the mask that does not hold the cell
+        // decides for itself, one cell after the other, from a copy of the
+        // cell parked in the free upper half of the interaction list
+        const uint32_t bm = __ballot_sync(kFull, mixed);
+        const uint32_t mrank = __popc(bm & lanes_below);
+        if (mixed) {
+            list[32u + mrank] = make_float4(com.x, com.y, g * chm.w, two_half);
+            s_mix[warp][mrank][0] = R;
+        }
+        __syncwarp();
+        const uint32_t nm = __popc(bm);
+        for (uint32_t i = 0; i < nm; ++i) {
+            const float4 cf = list[32u + i];
+            const bool active = (s_mix[warp][i][0] & lane_bit) != 0u;
+            const float dx = cf.x - tx, dy = cf.y - ty;
+            const bool approx = active && approximates(cf.w, dist2(dx, dy));
+            term(dx, dy, cf.z, approx);
+            const uint32_t O = __ballot_sync(kFull, active && !approx);
+            if (lane == 0) s_mix[warp][i][1] = O;
+        }
+        __syncwarp();
+        if (mixed) op |= s_mix[warp][mrank][1];
+
+        // leaves of several bodies: each body summed directly, self excluded
+        uint32_t bl = __ballot_sync(kFull, multi);
+        while (bl) {
+            const uint32_t src = __ffs(bl) - 1u;
+            bl &= bl - 1u;
+            const uint32_t start = __shfl_sync(kFull, rd.x, src);
+            const uint32_t end = __shfl_sync(kFull, rd.y, src);
+            const uint32_t M = __shfl_sync(kFull, A, src);
+            const bool active = (M >> lane) & 1u;
+            if (end > n) set_err(err, kErrPackedIndex);
+            for (uint32_t j = start; j < min(end, n); ++j) {
+                const float4 b = __ldg(reinterpret_cast<const float4*>(
+                    bodies[__ldg(&entries[j].data[1])].position_mass));
+                term(b.x - tx, b.y - ty, g * b.z, active && j != p);
+            }
+        }
+
+        // append the list terms, push the opened cells in lane order
+        const uint32_t la = __ballot_sync(kFull, ap != 0u);
+        if (ap) list[nlist + __popc(la & lanes_below)] = make_float4(ex, ey, g * em,
+                                                                      __uint_as_float(ap));
+        nlist += __popc(la);
+        const uint32_t lp = __ballot_sync(kFull, op != 0u);
+        if (len + __popc(lp) > kPkStack) {  // deeper than the bound: walk again cell by cell
+            overflow = true;
+            break;
+        }
+        if (op) stack[len + __popc(lp & lanes_below)] = make_uint2(c, op);
+        len += __popc(lp);
+        __syncwarp();
+        if (nlist >= 32u) {
+            flush(nlist);
+            nlist = 0;
+            __syncwarp();
+        }
+    }
+    if (overflow) {
+        __syncwarp();
+        packed_walk_cellwise(st, bodies, entries, cells, n, ncells, ti, tx, ty, p, valid, s_cell,
+                             s_cell + kPackedStack, err, &ax, &ay);
+    } else {
+        flush(nlist);
+    }
+    if (valid) accel[ti] = make_float4(ax, ay, 0.f, 0.f);
 }
 
 // ============================================================ export =====
@@ -2263,9 +2499,12 @@ cudaError_t launch_traverse_packed(const BhSettings* settings, const GpuBody* bo
                                    const GpuEntry* entries, const GpuCell* cells, uint32_t n,
                                    uint32_t ncells, float4* accel, uint32_t* err,
                                    cudaStream_t s) {
+    // err[1]: set when the entries and bodies disagree (the walk then goes
+    // cell by cell)
+    k_check_packed<<<(n + 255) / 256, 256, 0, s>>>(bodies, entries, n, err + 1);
     const uint32_t warps = (n + 31) / 32;
-    k_traverse_packed<<<(warps + 7) / 8, 256, 0, s>>>(settings, bodies, entries, cells, n, ncells,
-                                                      accel, err);
+    k_traverse_packed<<<(warps + kPkWarps - 1) / kPkWarps, kPkWarps * 32, 0, s>>>(
+        settings, bodies, entries, cells, n, ncells, accel, err, err + 1);
     return cudaGetLastError();
 }
 

@@ -233,7 +233,8 @@ int galaxy_bh_tree_footprint(uint32_t n, const bh_config* cfg, uint64_t* bytes);
 /* ---- BH #2B1 host-tree path -----------------------------------------------
  * NbodyGpu::traverse (nbody_gpu.rs:640-780) over a packed flat tree
  * (pack_flat_tree, nbody_gpu.rs:175-250): uploads, traverses with the
- * reference's f32 MAC, and reads back n accelerations. */
+ * reference's f32 MAC (each body's decisions and terms are the reference's;
+ * their summation order differs), and reads back n accelerations. */
 int galaxy_bh_traverse_packed(bh_device* dev, const BhSettings* settings, const GpuBody* bodies,
                               uint32_t n, const GpuEntry* entries, const GpuCell* cells,
                               uint32_t cell_count, GpuAccel* out, bh_stage_timing* timing);
