@@ -1833,19 +1833,22 @@ __global__ void __launch_bounds__(kPkWarps * 32) k_traverse_packed(
     const float theta = st.physics[0], soft = st.physics[1], g = st.physics[2];
     const uint32_t p = p0 + lane;
     const bool valid = p < n;
-    const uint32_t ti = valid ? entries[p].data[1] : 0u;
-    const bool ti_ok = ti < n;
-    const GpuBody tb = (valid && ti_ok) ? bodies[ti] : GpuBody{};
-    const float tx = tb.position_mass[0], ty = tb.position_mass[1];
     uint32_t* s_cell = reinterpret_cast<uint32_t*>(s_stack[warp]);
     float ax = 0.f, ay = 0.f;
     if (*inconsistent) {
-        packed_walk_cellwise(st, bodies, entries, cells, n, ncells, ti, tx, ty, tb.meta[0],
-                             valid && ti_ok, s_cell, s_cell + kPackedStack, err, &ax, &ay);
-        if (valid && ti_ok) accel[ti] = make_float4(ax, ay, 0.f, 0.f);
+        // the reference's own indexing: lane p walks for body p, at the
+        // Morton position that body records
+        const GpuBody b = valid ? bodies[p] : GpuBody{};
+        packed_walk_cellwise(st, bodies, entries, cells, n, ncells, p, b.position_mass[0],
+                             b.position_mass[1], b.meta[0], valid, s_cell,
+                             s_cell + kPackedStack, err, &ax, &ay);
+        if (valid) accel[p] = make_float4(ax, ay, 0.f, 0.f);
         return;
     }
-    // consistent input: every valid lane's body is ti, at position p
+    // consistent input: the body at position p is ti, and it records p
+    const uint32_t ti = valid ? entries[p].data[1] : 0u;
+    const GpuBody tb = valid ? bodies[ti] : GpuBody{};
+    const float tx = tb.position_mass[0], ty = tb.position_mass[1];
     const float eps2 = soft * soft;
     const uint32_t valid_mask = __ballot_sync(kFull, valid);
     const uint32_t lanes_below = (1u << lane) - 1u;

@@ -304,6 +304,39 @@ def test_packed_path_matches_models(gpu, oracle):
         assert np.quantile(rel_ref, 0.999) < 1e-5
 
 
+def test_packed_path_inconsistent_records_follow_the_reference(gpu, oracle):
+    """Packed records whose bodies and entries disagree (two bodies record
+    each other's Morton positions, so a body's own-cell test no longer
+    matches its entry) cannot use the lane bit of a position for
+    self-exclusion: the traversal then walks cell by cell, one body per lane
+    in body order, exactly as the reference's kernel indexes its targets
+    (barnes_hut_flat.cu:65-146), and still matches the f32 model of that
+    kernel on the same records."""
+    bodies = oracle.make_disc(3000, 303, 5.0e10, 3.0)
+    oc = oracle.Config()
+    b32 = f32_bodies(bodies)
+    ot = oracle.build_flat_tree(b32, oc)
+    packed = pack_flat_tree(b32, ot, Config())
+    op = oracle.pack_flat_tree(b32, ot, oc)
+    consistent = gpu.traverse(packed).accelerations
+    i, j = int(op.entries[10, 1]), int(op.entries[2000, 1])
+    for rec in (packed.bodies.view(np.uint32).reshape(-1, 8), op.bodies):
+        rec[i, 4], rec[j, 4] = rec[j, 4], rec[i, 4]
+    res = gpu.traverse(packed).accelerations
+    model = oracle.f32_traverse_packed(op)[:, :2].astype(np.float64)
+    rel = oracle.relative_errors(res, model)
+    assert np.quantile(rel, 0.99) < 1e-5
+    # the two bodies whose own-cell tests moved change; the others do not
+    others = np.ones(len(res), bool)
+    others[[i, j]] = False
+    rel_cons = oracle.relative_errors(res[others], consistent[others])
+    assert np.quantile(rel_cons, 0.99) < 1e-5
+    if oracle.ref_cuda() is not None:
+        ref_gpu, _ = oracle.ref_cuda_traverse(op)
+        rel_ref = oracle.relative_errors(res, ref_gpu[:, :2].astype(np.float64))
+        assert np.quantile(rel_ref, 0.999) < 1e-5
+
+
 def test_repeat_rebuild_bit_identical(gpu, rt, oracle):
     cfg = Config(theta=0.5, softening_kpc=0.01, g=1.0, bucket=1)
     bodies = scenarios.binary_encounter(40000, 9)
