@@ -486,6 +486,16 @@ def run_engine(args, world, rank, local, pg):
     rt = ParallelTreeRuntime(gpu)
     cfg = Config(theta=THETA, softening_kpc=EPS, g=G, bucket=BUCKET, max_depth=48)
     bodies, s0 = f32_workload()
+    if args.only_same_tree:
+        # the same-tree kernel timings alone (for profilers)
+        kernels = same_tree_kernels(gpu, rt, s0, cfg)
+        if rank == 0:
+            print(json.dumps({"same_tree_kernels": kernels, "only_same_tree": True,
+                              "config": config_dict(world)}), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     ev, _ = gpu.create_evolving_state_records(s0)
     tree = rt.create_tree(gpu, ev, cfg)
     rt.rebuild(gpu, ev, tree, cfg)
@@ -1123,6 +1133,9 @@ def main():
     ap.add_argument("--only-step", action="store_true",
                     help="run the timed steps of the headline workload and nothing else "
                          "(a short line without the side legs; for profilers)")
+    ap.add_argument("--only-same-tree", action="store_true",
+                    help="time this engine's kernels on the workload's initial tree and "
+                         "nothing else (for profilers)")
     args = ap.parse_args()
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
