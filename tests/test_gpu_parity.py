@@ -304,6 +304,31 @@ def test_packed_path_matches_models(gpu, oracle):
         assert np.quantile(rel_ref, 0.999) < 1e-5
 
 
+@pytest.mark.parametrize("scenario,theta", [("cold", 0.5), ("cold", 0.12), ("binary", 0.7)])
+def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta):
+    """The lane-parallel packed walk on a 2^16-body tree (deep enough for
+    mixed cells, list flushes and every box outcome): each body's terms are
+    the reference's (barnes_hut_flat.cu:65-146), so against the f32 model of
+    that kernel on the same records only the summation order differs."""
+    n = 1 << 16
+    bodies = (scenarios.cold_disc(n, 5) if scenario == "cold"
+              else scenarios.binary_encounter(n, 13))
+    b32 = f32_bodies(bodies)
+    oc = oracle.Config(theta=theta, softening=0.005, g=1.0, bucket=1, max_depth=48)
+    ot = oracle.build_flat_tree(b32, oc)
+    cfg = Config(theta=theta, softening_kpc=0.005, g=1.0, bucket=1, max_depth=48)
+    packed = pack_flat_tree(b32, ot, cfg)
+    op = oracle.pack_flat_tree(b32, ot, oc)
+    res = gpu.traverse(packed).accelerations
+    model = oracle.f32_traverse_packed(op)[:, :2].astype(np.float64)
+    rel = oracle.relative_errors(res, model)
+    assert np.median(rel) < 1e-6 and np.quantile(rel, 0.99) < 1e-5
+    if oracle.ref_cuda() is not None:
+        ref_gpu, _ = oracle.ref_cuda_traverse(op)
+        rel_ref = oracle.relative_errors(res, ref_gpu[:, :2].astype(np.float64))
+        assert np.median(rel_ref) < 1e-6 and np.quantile(rel_ref, 0.99) < 1e-5
+
+
 def test_packed_path_inconsistent_records_follow_the_reference(gpu, oracle):
     """Packed records whose bodies and entries disagree (two bodies record
     each other's Morton positions, so a body's own-cell test no longer
