@@ -304,12 +304,22 @@ def test_packed_path_matches_models(gpu, oracle):
         assert np.quantile(rel_ref, 0.999) < 1e-5
 
 
+# median / p99 relative difference allowed between two f32 summation orders
+# of the same terms.  The reference's own f32 depth-first sum is itself that
+# far from the exact sum of its terms (a CPU replay of 150 bodies of this
+# cold disc: median 4.6e-7 / p90 1.7e-6 / max 1.8e-5 at theta 0.5 with ~220
+# terms a body, 1.2e-6 / 4.0e-6 / 5.0e-5 at theta 0.12 with ~2,300).
+PACKED_ORDER_TOLERANCE = {0.5: (1e-6, 1e-5), 0.7: (1e-6, 1e-5), 0.12: (4e-6, 1e-4)}
+
+
 @pytest.mark.parametrize("scenario,theta", [("cold", 0.5), ("cold", 0.12), ("binary", 0.7)])
 def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta):
     """The lane-parallel packed walk on a 2^16-body tree (deep enough for
     mixed cells, list flushes and every box outcome): each body's terms are
     the reference's (barnes_hut_flat.cu:65-146), so against the f32 model of
-    that kernel on the same records only the summation order differs."""
+    that kernel on the same records only the summation order differs, by the
+    f32 rounding of sums of that many terms."""
+    med, p99 = PACKED_ORDER_TOLERANCE[theta]
     n = 1 << 16
     bodies = (scenarios.cold_disc(n, 5) if scenario == "cold"
               else scenarios.binary_encounter(n, 13))
@@ -322,11 +332,11 @@ def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta):
     res = gpu.traverse(packed).accelerations
     model = oracle.f32_traverse_packed(op)[:, :2].astype(np.float64)
     rel = oracle.relative_errors(res, model)
-    assert np.median(rel) < 1e-6 and np.quantile(rel, 0.99) < 1e-5
+    assert np.median(rel) < med and np.quantile(rel, 0.99) < p99
     if oracle.ref_cuda() is not None:
         ref_gpu, _ = oracle.ref_cuda_traverse(op)
         rel_ref = oracle.relative_errors(res, ref_gpu[:, :2].astype(np.float64))
-        assert np.median(rel_ref) < 1e-6 and np.quantile(rel_ref, 0.99) < 1e-5
+        assert np.median(rel_ref) < med and np.quantile(rel_ref, 0.99) < p99
 
 
 def test_packed_path_inconsistent_records_follow_the_reference(gpu, oracle):
