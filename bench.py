@@ -736,6 +736,9 @@ def run_engine(args, world, rank, local, pg):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "traffic": BUILD_DRAM_BYTES_PER_STEP,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "step's sort, build and leapfrog kernels on this workload "
+                                       "(one capture, per step)",
                      "kernels": "sort/build/leapfrog (integrate+bounds, morton, 4 radix "
                                 "passes, count/scan, cells, aggregate)",
                      "peak_source": peaks["source"],
