@@ -808,7 +808,12 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
 #endif
 constexpr uint32_t kAggBlockPositions = GBH_AGG_POSITIONS;
 constexpr uint32_t kCellsThreads = 256;
-constexpr uint32_t kCellsWin = 1024;
+// 512 positions: wider windows load more than their searches save (1024 and
+// 2048 measured slower at 2^20 and 2^24)
+#ifndef GBH_CELLS_WIN
+#define GBH_CELLS_WIN 512
+#endif
+constexpr uint32_t kCellsWin = GBH_CELLS_WIN;
 constexpr uint32_t kMaxChain = kMortonDepth + 1;  // cells per position: depths 0..16
 
 #ifndef GBH_CELLS_KARY
