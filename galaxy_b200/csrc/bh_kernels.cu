@@ -807,7 +807,10 @@ __global__ void __launch_bounds__(kScanThreads) k_count_scan(
 #define GBH_AGG_POSITIONS 256
 #endif
 constexpr uint32_t kAggBlockPositions = GBH_AGG_POSITIONS;
-constexpr uint32_t kCellsThreads = 256;
+#ifndef GBH_CELLS_THREADS
+#define GBH_CELLS_THREADS 256
+#endif
+constexpr uint32_t kCellsThreads = GBH_CELLS_THREADS;  // positions (and threads) per block
 // 512 positions: wider windows load more than their searches save (1024 and
 // 2048 measured slower at 2^20 and 2^24)
 #ifndef GBH_CELLS_WIN
