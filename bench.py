@@ -486,6 +486,20 @@ def run_engine(args, world, rank, local, pg):
     rt = ParallelTreeRuntime(gpu)
     cfg = Config(theta=THETA, softening_kpc=EPS, g=G, bucket=BUCKET, max_depth=48)
     bodies, s0 = f32_workload()
+    if args.only_batched:
+        # the batched leg alone (for profilers; its timed steps sit in an
+        # NVTX range "batched")
+        batched = run_batched_leg(gpu, steps=min(args.steps, 20), warmup=args.warmup, pg=pg,
+                                  rank=rank, world=world)
+        if rank == 0:
+            print(json.dumps({"batched": {k: batched[k] for k in
+                                          ("bodies", "steps", "ms_per_step", "value",
+                                           "speedup_vs_plain")},
+                              "only_batched": True}), flush=True)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     if args.only_same_tree:
         # the same-tree kernel timings alone (for profilers)
         kernels = same_tree_kernels(gpu, rt, s0, cfg)
@@ -863,16 +877,18 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
                                  probes=128)
     tuned_cfgs = tuning.configs([s.count for s in states], [cfg] * len(states))
 
-    def timed(cfgs, bits, warps, run_states):
+    def timed(cfgs, bits, warps, run_states, label):
         batch = Batch(gpu, run_states, cfgs)
         batch.tune(bits, warps)
         batch.solve()
         batch.step(1e-3, max(warmup, 3))
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push(label)  # ncu --nvtx --nvtx-include <label>/
         e0.record(stream)
         batch.step(1e-3, steps)
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         ms = shard.max_over_ranks(pg, e0.elapsed_time(e1), "cuda")
         arena = batch.arena_bytes()
         batch.close()
@@ -880,10 +896,10 @@ def run_batched_leg(gpu, steps: int, warmup: int, count: int = 512, plain_steps:
 
     untuned_states = [gpu.create_evolving_state_records(gpu.read_evolving_state_records(s)[0])[0]
                       for s in states]
-    u_ms, _ = timed([cfg] * len(states), 8, 4, untuned_states)
+    u_ms, _ = timed([cfg] * len(states), 8, 4, untuned_states, "batched_untuned")
     for s in untuned_states:
         s.close()
-    b_ms, arena = timed(tuned_cfgs, tuning.radix_bits, tuning.traverse_warps, states)
+    b_ms, arena = timed(tuned_cfgs, tuning.radix_bits, tuning.traverse_warps, states, "batched")
     # plain path, simulation after simulation (a prefix of the plan when
     # plain_sims is set; the rate is per body-step either way)
     rt = ParallelTreeRuntime(gpu)
@@ -1136,6 +1152,8 @@ def main():
     ap.add_argument("--only-step", action="store_true",
                     help="run the timed steps of the headline workload and nothing else "
                          "(a short line without the side legs; for profilers)")
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run the mixed-size batched leg and nothing else (for profilers)")
     ap.add_argument("--only-same-tree", action="store_true",
                     help="time this engine's kernels on the workload's initial tree and "
                          "nothing else (for profilers)")
