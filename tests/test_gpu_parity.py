@@ -312,10 +312,12 @@ def test_packed_path_matches_models(gpu, oracle):
 PACKED_ORDER_TOLERANCE = {0.5: (1e-6, 1e-5), 0.7: (1e-6, 1e-5), 0.12: (4e-6, 1e-4)}
 
 
-@pytest.mark.parametrize("scenario,theta", [("cold", 0.5), ("cold", 0.12), ("binary", 0.7)])
-def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta):
+@pytest.mark.parametrize("scenario,theta,bucket", [("cold", 0.5, 1), ("cold", 0.12, 1),
+                                                   ("binary", 0.7, 1), ("binary", 0.5, 8)])
+def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta, bucket):
     """The lane-parallel packed walk on a 2^16-body tree (deep enough for
-    mixed cells, list flushes and every box outcome): each body's terms are
+    mixed cells, list flushes and every box outcome; leaves of up to 8
+    bodies in the last case): each body's terms are
     the reference's (barnes_hut_flat.cu:65-146), so against the f32 model of
     that kernel on the same records only the summation order differs, by the
     f32 rounding of sums of that many terms."""
@@ -324,9 +326,9 @@ def test_packed_path_lane_parallel_walk_at_scale(gpu, oracle, scenario, theta):
     bodies = (scenarios.cold_disc(n, 5) if scenario == "cold"
               else scenarios.binary_encounter(n, 13))
     b32 = f32_bodies(bodies)
-    oc = oracle.Config(theta=theta, softening=0.005, g=1.0, bucket=1, max_depth=48)
+    oc = oracle.Config(theta=theta, softening=0.005, g=1.0, bucket=bucket, max_depth=48)
     ot = oracle.build_flat_tree(b32, oc)
-    cfg = Config(theta=theta, softening_kpc=0.005, g=1.0, bucket=1, max_depth=48)
+    cfg = Config(theta=theta, softening_kpc=0.005, g=1.0, bucket=bucket, max_depth=48)
     packed = pack_flat_tree(b32, ot, cfg)
     op = oracle.pack_flat_tree(b32, ot, oc)
     res = gpu.traverse(packed).accelerations
